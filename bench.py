@@ -1,0 +1,366 @@
+#!/usr/bin/env python
+"""Throughput of the HydroC Godunov/MUSCL time step on B200.
+
+Workload (default): the 4096 x 4096 centred blast in FP64 -- rho = 1, u = v = 0,
+E = 1e-5, E = 1/dx^2 in the centre cell, dx = 1/4096, gamma 1.4, reflecting
+walls, MUSCL, iorder 2, slope_type 1, niter_riemann 10, courant_factor 0.8 --
+advanced K time steps from its initial state (steps 0..K-1; the workload's
+run is 200 steps).  One step = both dimension-split sweeps plus the CFL dt
+(recomputed on even steps), as in the reference driver loop.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line.  `value` is Mcell-updates/s (cells x steps / s) over
+all ranks with the state resident in HBM, timed with CUDA events on the
+library's stream; `e2e` is the same metric through the reference entry
+points (compute_deltat + hydro_godunov) on a pinned host array, with the
+upload, the per-step dt reads and the final download inside the timed region.
+With N > 1 (torchrun) every rank advances its own replica (weak scaling; the
+north-star workload is one grid on one GPU, so there is no exchange).
+
+--impl reference times the reference's own C99/OpenMP implementation of the
+same step on the host cores (oracle/_ref, compiled from the reference
+sources) on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "c1": dict(name="hydroc_4096x4096_centre_blast_fp64", nx=4096, ny=4096, testcase=0,
+               run_steps=200),
+    "c0": dict(name="hydroc_250x125_corner_blast_fp64", nx=250, ny=125, testcase=1,
+               run_steps=100),
+}
+BYTES_PER_CELL_SWEEP = 64   # 4 doubles read + 4 doubles written per cell and sweep
+BYTES_PER_CELL_STEP = 2 * BYTES_PER_CELL_SWEEP
+
+
+def env_int(k, d):
+    try:
+        return int(os.environ.get(k, d))
+    except ValueError:
+        return d
+
+
+def measured_peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic_per_launch():
+    """DRAM bytes per sweep launch from the committed ncu summary (if any)."""
+    p = os.path.join(ROOT, "profiles", "sweep_fp64_4096_traffic.txt")
+    try:
+        for line in open(p):
+            if line.startswith("dram_bytes_per_launch_full_size:"):
+                return float(line.split(":", 1)[1].split()[0])
+    except Exception:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi samples (SM clock, throttle reasons) while it runs."""
+
+    QUERY = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "50"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return self
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append((time.time(), [x.strip() for x in line.split(",")]))
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=5)
+
+    def summary(self, t0, t1):
+        rows = [s for (ts, s) in self.samples if t0 - 0.05 <= ts <= t1 + 0.05] or \
+               [s for (_, s) in self.samples]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        smax = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4)
+                          if len(r) > 4 + i and r[4 + i].lower().startswith("active")})
+        pw = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": reasons,
+                "power_w_max": max(pw) if pw else None, "samples": len(rows)}
+
+
+def dist_setup(gpus):
+    world = env_int("WORLD_SIZE", 1)
+    rank = env_int("RANK", 0)
+    local = env_int("LOCAL_RANK", 0)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("nccl" if gpus else "gloo",
+                                timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    return world, rank, local, pg
+
+
+def all_max(pg, x, device):
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg, device):
+    if pg is not None:
+        import torch
+        pg.all_reduce(torch.zeros(1, device=device))
+
+
+def cpu_reference_sample(wl, budget_s, max_steps, warm=1):
+    """The reference's own C99/OpenMP code (oracle/_ref) on the host cores,
+    falling back to the C restatement (oracle/_build) where the reference was
+    not compiled.  Runs whole time steps of the workload from its initial
+    state until budget_s is spent (at least one timed step)."""
+    from oracle import oracle as O
+    p = O.make_param(wl["nx"], wl["ny"], boundary=(1, 1, 1, 1))
+    cores = os.cpu_count() or 1
+    O.oracle_lib().orc_set_threads(cores)
+    if O.ref_available():
+        kind = "reference"
+        r = O.RefState(p, wl["testcase"], nxystep=256)
+        t0 = time.perf_counter()
+        r.run(warm)
+        tw = time.perf_counter() - t0
+        nrun = max(1, min(max_steps, int(budget_s / max(tw / max(warm, 1), 1e-6))))
+        n, dts, _, mcs_avg, el = r.run(warm + nrun)
+        r.close()
+        desc = (f"reference C99/OpenMP (oracle/_ref, gcc -O3 -fopenmp -mavx2) on "
+                f"{wl['nx']}x{wl['ny']}: steps {warm}..{warm + n - 1} after {warm} warm-up "
+                f"step(s), {cores} OpenMP threads")
+    else:
+        kind = "port"
+        u = O.init_state(p, wl["testcase"])
+        t0 = time.perf_counter()
+        n, _, _ = O.run(p, u, max(1, min(max_steps, 2)))
+        el = time.perf_counter() - t0
+        desc = (f"C restatement (oracle/_build, OpenMP over lines) on {wl['nx']}x{wl['ny']}: "
+                f"{n} steps, {cores} threads")
+    mcs = wl["nx"] * wl["ny"] * n / el / 1e6
+    return {"value": round(mcs, 3), "unit": "Mcell-updates/s", "cores": cores, "kind": kind,
+            "sample": desc, "steps": n, "seconds": round(el, 3)}
+
+
+def run_reference_arm(args, wl):
+    world, rank, local, pg = dist_setup(False)
+    if rank != 0:
+        return 0
+    budget = float(os.environ.get("HYDRO_BENCH_REF_BUDGET_S", "90"))
+    cpu = cpu_reference_sample(wl, budget, args.steps, warm=max(1, min(args.warmup, 3)))
+    line = {
+        "impl": "reference", "metric": "Mcell-updates/s", "value": cpu["value"],
+        "unit": "Mcell-updates/s", "n_gpus": 0, "steps": cpu["steps"], "warmup": args.warmup,
+        "ms_per_step": round(cpu["seconds"] / max(cpu["steps"], 1) * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (the workload's initial condition, generated in-process)",
+        "config": {"workload": wl["name"], "nx": wl["nx"], "ny": wl["ny"],
+                   "testcase": wl["testcase"], "steps_requested": args.steps,
+                   "parallelism": f"OpenMP {cpu['cores']} threads"},
+        "cpu_baseline": {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "e2e": {"value": cpu["value"], "unit": "Mcell-updates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c1")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    wl = WORKLOADS[args.workload]
+    if args.warmup < 3:
+        print("warning: --warmup < 3", file=sys.stderr)
+    if args.impl == "reference":
+        return run_reference_arm(args, wl)
+
+    import torch
+    world, rank, local, pg = dist_setup(True)
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+
+    import hydro_b200
+    from hydro_b200 import Domain, HydroRun, init_state, make_params
+    lib = hydro_b200.load()
+    if lib.hydro_b200_set_device(local) != 0:
+        hydro_b200._lib.check()
+
+    nx, ny, K, W = wl["nx"], wl["ny"], args.steps, args.warmup
+    H = make_params(nx, ny, testcase=wl["testcase"])
+    u0 = init_state(H)
+    state_bytes = u0.nbytes
+    dom = Domain(H)
+    stream = torch.cuda.ExternalStream(dom.stream_ptr, device=device)
+
+    # Warm-up: W steps of the workload (module load, clocks), then back to step 0.
+    dom.upload(u0)
+    dom.set_clock()
+    dom.launch_steps(W)
+    dom.synchronize()
+    dom.upload(u0)
+    dom.set_clock()
+
+    sampler = ClockSampler(local).start()
+    time.sleep(0.3)
+    barrier(pg, device)
+    torch.cuda.synchronize(device)
+    dom.synchronize()
+    launches0 = dom.launch_count
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    tw0 = time.time()
+    e0.record(stream)
+    dom.launch_steps(K)
+    e1.record(stream)
+    e1.synchronize()
+    tw1 = time.time()
+    dom.synchronize()
+    torch.cuda.synchronize(device)
+    barrier(pg, device)
+    ms = e0.elapsed_time(e1)
+    gpu_launches = dom.launch_count - launches0
+    sampler.stop()
+    clocks = sampler.summary(tw0, tw1)
+    ms_max = all_max(pg, ms, device)
+    t_end, n_end, dt_end = dom.get_clock()
+    assert n_end == K, (n_end, K)
+    value = world * nx * ny * K / (ms_max / 1e3) / 1e6
+
+    # Per-launch duration of the sweep kernel: the same K steps again with an
+    # event pair around every sweep launch.
+    dom.upload(u0)
+    dom.set_clock()
+    dom.profile(True)
+    dom.profile_read(reset=True)
+    dom.launch_steps(K)
+    msx, msy, nxl, nyl = dom.profile_read(reset=True)
+    dom.profile(False)
+    sweep_ms = (msx + msy) / max(nxl + nyl, 1)
+    alg_bytes = BYTES_PER_CELL_SWEEP * nx * ny
+    achieved = alg_bytes / (sweep_ms / 1e3) / 1e9
+    peak, peak_kind = measured_peak_hbm()
+    dom.close()
+
+    # End to end through the reference entry points on a pinned host array.
+    e2e = None
+    if not args.no_e2e:
+        pinned = torch.empty(u0.shape, dtype=torch.float64, pin_memory=True)
+        host = pinned.numpy()
+        host[...] = u0
+        run = HydroRun(H, host)
+        est = torch.cuda.ExternalStream(run.stream_ptr, device=device)  # creates the mirror
+        barrier(pg, device)
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(est)
+        run.sync_to_device()
+        run.run_host_loop(K)
+        run.sync_to_host()
+        f1.record(est)
+        f1.synchronize()
+        e2e_ms = all_max(pg, f0.elapsed_time(f1), device)
+        run.close()
+        e2e = {"value": round(world * nx * ny * K / (e2e_ms / 1e3) / 1e6, 3),
+               "unit": "Mcell-updates/s",
+               "h2d_bytes_per_step": round(state_bytes / K, 1),
+               "d2h_bytes_per_step": round((state_bytes + 16 * ((K + 1) // 2)) / K, 1),
+               "path": "compute_deltat + hydro_godunov (reference ABI) on a pinned host uold; "
+                       "upload, per-even-step Courant read-back and final download timed"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        budget = float(os.environ.get("HYDRO_BENCH_CPU_BUDGET_S", "20"))
+        cpu = cpu_reference_sample(wl, budget, 50, warm=1)
+        cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+
+    if pg is not None:
+        barrier(pg, device)
+        pg.destroy_process_group()
+    if rank != 0:
+        return 0
+    traffic = ncu_traffic_per_launch()
+    line = {
+        "metric": "Mcell-updates/s", "value": round(value, 3), "unit": "Mcell-updates/s",
+        "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": round(ms_max / K, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (the workload's initial condition, generated in-process)",
+        "config": {"workload": wl["name"], "nx": nx, "ny": ny, "testcase": wl["testcase"],
+                   "steps": f"0..{K - 1} of the {wl['run_steps']}-step run",
+                   "precision": "fp64 (bitwise equal to the reference)",
+                   "parallelism": "replicas" if world > 1 else "single GPU",
+                   "l2": f"state {state_bytes / 1e6:.1f} MB per buffer > 126 MB L2; no flush"},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                     "unit": "GB/s", "frac": round(achieved / peak, 4),
+                     "traffic": traffic, "kernel": "hb::sweep_kernel (x and y sweeps)",
+                     "alg_bytes_per_launch": alg_bytes, "launch_ms": round(sweep_ms, 4),
+                     "peak_kind": peak_kind},
+        "gpu_launches": gpu_launches,
+        "clocks": clocks,
+        "e2e": e2e,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

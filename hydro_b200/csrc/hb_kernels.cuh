@@ -1,0 +1,52 @@
+// hb_kernels.cuh -- kernel argument records and launchers shared by the
+// host runtime (hb_runtime.cu) and the kernels (hb_kernels.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "hb_stages.cuh"
+
+namespace hb {
+
+// Device-resident clock of the multi-step driver (main.c:344-408 state).
+struct DevClock {
+    double t, dt, tend;
+    int nstep, nstepmax;
+    int nstep0;   // nstep when the clock was last set (index base of dts)
+    int active;   // 0 once t >= tend or nstep >= nstepmax
+    double* dts;  // optional per-step dt record
+    int ndts;
+};
+
+// One fused sweep over every interior line of a direction.
+struct SweepArgs {
+    const double* in;        // interior cells are read here
+    const double* resid;     // the resident state: ghost cells are read (and sourced) here
+                             // when they are not interior cells
+    double* out;             // updated interior cells are written here
+    double* gout;            // ghost cells of the swept direction are written here (or null)
+    const DevClock* clk;     // null: use dt below; else dt and the active flag come from here
+    double dt;
+    unsigned long long* courant;  // null or [2]: fused max(c+|u|), max(c+|v|) (bit patterns)
+    int nx, ny, nxt, nyt;
+    long long vs;            // nxt * nyt (stride between variables)
+    int bnd_lo, bnd_hi;      // boundary types of the swept direction (left/right or down/up)
+    int seg;                 // output cells per thread segment
+    int nlines;              // interior lines (ny for the x sweep, nx for the y sweep)
+    int n;                   // cells along a line including ghosts (nxt or nyt)
+};
+
+constexpr int kSweepThreads = 128;
+
+// Launchers (hb_kernels.cu).  Each returns the cudaError_t of the launch.
+cudaError_t launch_sweep(int dir, const SweepArgs& a, const Phys& P, cudaStream_t s);
+cudaError_t launch_courant(const double* u, int nx, int ny, int nxt, long long vs, const Phys& P,
+                           unsigned long long* cour, cudaStream_t s);
+cudaError_t launch_boundary(double* u, int idim, int nx, int ny, int nxt, int nyt, long long vs,
+                            int bnd_lo, int bnd_hi, cudaStream_t s);
+cudaError_t launch_clock_begin(DevClock* c, unsigned long long* cour, double courant_factor,
+                               double dx, double smallc, cudaStream_t s);
+cudaError_t launch_clock_end(DevClock* c, cudaStream_t s);
+
+}  // namespace hb

@@ -1,0 +1,615 @@
+// hb_runtime.cu -- host runtime and C ABI of libhydro_b200.so.
+//
+// Layers:
+//   hb_domain          a device-resident state (reference layout), its scratch
+//                      buffer, Courant accumulators, device clock and stream;
+//   reference ABI      hydro_godunov / compute_deltat / make_boundary / ... with
+//                      the reference's signatures, mapping Hv->uold to a
+//                      domain through a registry (device mirror of host memory);
+//   hydro_b200_*       residency control, the device-resident driver loop,
+//                      errors, and the domain (device pointer) API.
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstddef>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/hydro_b200.h"
+#include "hb_kernels.cuh"
+
+using hb::DevClock;
+using hb::Phys;
+using hb::SweepArgs;
+
+// ---------------------------------------------------------------- errors
+static thread_local int g_err = HB_OK;
+static thread_local char g_msg[512] = "";
+
+static bool strict_mode() {
+    const char* s = getenv("HYDRO_B200_STRICT");
+    return s && s[0] == '1';
+}
+
+static int set_error(int code, const char* fmt, ...) {
+    g_err = code;
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_msg, sizeof(g_msg), fmt, ap);
+    va_end(ap);
+    if (strict_mode()) {
+        fprintf(stderr, "hydro_b200: error %d: %s\n", code, g_msg);
+        abort();
+    }
+    return code;
+}
+
+#define HB_CU(call)                                                                      \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess)                                                           \
+            return set_error(e_ == cudaErrorMemoryAllocation ? HB_ERR_NOMEM : HB_ERR_CUDA, \
+                             "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_),     \
+                             __FILE__, __LINE__);                                        \
+    } while (0)
+
+extern "C" int hydro_b200_last_error(void) { return g_err; }
+extern "C" const char* hydro_b200_last_error_message(void) { return g_msg; }
+extern "C" void hydro_b200_clear_error(void) {
+    g_err = HB_OK;
+    g_msg[0] = 0;
+}
+
+// ---------------------------------------------------------------- domain
+struct hb_domain {
+    int nx = 0, ny = 0, nxt = 0, nyt = 0;
+    long long vs = 0;
+    size_t nelem = 0;                  // 4 * nxt * nyt
+    double* A = nullptr;               // resident state
+    double* B = nullptr;               // scratch: output of the first sweep of a step
+    unsigned long long* cour = nullptr;  // [2] Courant maxima (bit patterns)
+    DevClock* clk = nullptr;
+    double* dts = nullptr;
+    int ndts = 0;
+    cudaStream_t stream = nullptr;
+    int device = 0;
+    Phys P{};
+    double courant_factor = 0.0;
+    int bnd_left = 1, bnd_right = 1, bnd_down = 1, bnd_up = 1;
+    bool cour_valid = false;  // cour holds the maxima of the current state
+    int h_nstep = 0;          // host view of the clock's nstep (parity of launches)
+    long long launches = 0;
+    // Optional event timing of every sweep launch (hydro_b200_domain_profile).
+    bool prof = false;
+    std::vector<cudaEvent_t> ev_pool;    // free events
+    std::vector<cudaEvent_t> ev_pending; // start/end pairs, sweep direction in ev_dir
+    std::vector<int> ev_dir;
+    double prof_ms[2] = {0.0, 0.0};
+    long long prof_n[2] = {0, 0};
+};
+
+static int validate(const hydroparam_t* H) {
+    if (!H) return set_error(HB_ERR_ARG, "null hydroparam_t");
+    if (H->nvar != 4)
+        return set_error(HB_ERR_ARG, "nvar=%d: only the reference's 4 variables are supported",
+                         H->nvar);
+    if (H->nx < 3 || H->ny < 3)
+        return set_error(HB_ERR_ARG, "grid %dx%d: nx and ny must be >= 3", H->nx, H->ny);
+    if ((H->nxt && H->nxt != H->nx + 4) || (H->nyt && H->nyt != H->ny + 4))
+        return set_error(HB_ERR_ARG, "nxt/nyt (%d,%d) must be nx+4, ny+4", H->nxt, H->nyt);
+    if (H->scheme < 1 || H->scheme > 3)
+        return set_error(HB_ERR_ARG, "scheme=%d: expected 1 (muscl), 2 (plmde) or 3 (collela)",
+                         H->scheme);
+    if (!(H->dx > 0.0)) return set_error(HB_ERR_ARG, "dx must be > 0");
+    if (H->niter_riemann < 0) return set_error(HB_ERR_ARG, "niter_riemann < 0");
+    if ((long long)(H->nx + 4) * (H->ny + 4) > (1ll << 31))
+        return set_error(HB_ERR_ARG, "grid too large for 32-bit line indices");
+    return HB_OK;
+}
+
+// Constants of the run, with the reference's formulas (see hb_stages.cuh).
+static void load_params(hb_domain* d, const hydroparam_t* H) {
+    Phys& P = d->P;
+    P.gamma = H->gamma;
+    P.gm1 = H->gamma - 1.0;
+    P.smallr = H->smallr;
+    P.smallc = H->smallc;
+    P.smallp = (H->smallc * H->smallc) / H->gamma;
+    P.gamma6 = (H->gamma + 1.0) / (2.0 * H->gamma);
+    P.smallpp = H->smallr * P.smallp;
+    P.entho = 1.0 / (H->gamma - 1.0);
+    P.slope_type = H->slope_type;
+    P.dx = H->dx;
+    P.niter = H->niter_riemann;
+    P.iorder = H->iorder;
+    P.scheme = H->scheme;
+    P.unit_slope = (H->slope_type == 1.0) ? 1 : 0;
+    d->courant_factor = H->courant_factor;
+    d->bnd_left = H->boundary_left;
+    d->bnd_right = H->boundary_right;
+    d->bnd_down = H->boundary_down;
+    d->bnd_up = H->boundary_up;
+}
+
+extern "C" void hydro_b200_domain_destroy(hb_domain* d) {
+    if (!d) return;
+    if (d->stream) cudaStreamSynchronize(d->stream);
+    for (cudaEvent_t e : d->ev_pool) cudaEventDestroy(e);
+    for (cudaEvent_t e : d->ev_pending) cudaEventDestroy(e);
+    cudaFree(d->A);
+    cudaFree(d->B);
+    cudaFree(d->cour);
+    cudaFree(d->clk);
+    cudaFree(d->dts);
+    if (d->stream) cudaStreamDestroy(d->stream);
+    delete d;
+}
+
+static int domain_alloc(hb_domain* d) {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return set_error(HB_ERR_NODEV, "no CUDA device visible");
+    HB_CU(cudaGetDevice(&d->device));
+    HB_CU(cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking));
+    HB_CU(cudaMalloc(&d->A, d->nelem * sizeof(double)));
+    HB_CU(cudaMalloc(&d->B, d->nelem * sizeof(double)));
+    HB_CU(cudaMalloc(&d->cour, 2 * sizeof(unsigned long long)));
+    HB_CU(cudaMalloc(&d->clk, sizeof(DevClock)));
+    HB_CU(cudaMemsetAsync(d->cour, 0, 2 * sizeof(unsigned long long), d->stream));
+    HB_CU(cudaMemsetAsync(d->clk, 0, sizeof(DevClock), d->stream));
+    return HB_OK;
+}
+
+extern "C" hb_domain* hydro_b200_domain_create(const hydroparam_t* H) {
+    if (validate(H) != HB_OK) return nullptr;
+    hb_domain* d = new hb_domain();
+    d->nx = H->nx;
+    d->ny = H->ny;
+    d->nxt = H->nx + 4;
+    d->nyt = H->ny + 4;
+    d->vs = (long long)d->nxt * d->nyt;
+    d->nelem = (size_t)4 * d->vs;
+    load_params(d, H);
+    if (domain_alloc(d) != HB_OK) {
+        hydro_b200_domain_destroy(d);
+        return nullptr;
+    }
+    return d;
+}
+
+extern "C" double* hydro_b200_domain_state(hb_domain* d) { return d ? d->A : nullptr; }
+extern "C" void* hydro_b200_domain_stream(hb_domain* d) { return d ? (void*)d->stream : nullptr; }
+extern "C" long long hydro_b200_domain_launch_count(hb_domain* d) { return d ? d->launches : 0; }
+
+extern "C" int hydro_b200_domain_upload(hb_domain* d, const double* host) {
+    if (!d || !host) return set_error(HB_ERR_ARG, "null domain or buffer");
+    HB_CU(cudaMemcpyAsync(d->A, host, d->nelem * sizeof(double), cudaMemcpyHostToDevice,
+                          d->stream));
+    d->cour_valid = false;
+    return HB_OK;
+}
+
+extern "C" int hydro_b200_domain_download(hb_domain* d, double* host) {
+    if (!d || !host) return set_error(HB_ERR_ARG, "null domain or buffer");
+    HB_CU(cudaMemcpyAsync(host, d->A, d->nelem * sizeof(double), cudaMemcpyDeviceToHost,
+                          d->stream));
+    return HB_OK;
+}
+
+extern "C" int hydro_b200_domain_synchronize(hb_domain* d) {
+    if (!d) return set_error(HB_ERR_ARG, "null domain");
+    HB_CU(cudaStreamSynchronize(d->stream));
+    return HB_OK;
+}
+
+// Fixed output-cell count per thread segment of the sweeps.
+static constexpr int kSeg = 64;
+
+static SweepArgs sweep_args(hb_domain* d, int dir, const double* in, double* out,
+                            const DevClock* clk, double dt, unsigned long long* cour) {
+    SweepArgs a;
+    a.in = in;
+    a.resid = d->A;
+    a.out = out;
+    a.gout = d->A;
+    a.clk = clk;
+    a.dt = dt;
+    a.courant = cour;
+    a.nx = d->nx;
+    a.ny = d->ny;
+    a.nxt = d->nxt;
+    a.nyt = d->nyt;
+    a.vs = d->vs;
+    if (dir == 1) {
+        a.bnd_lo = d->bnd_left;
+        a.bnd_hi = d->bnd_right;
+        a.nlines = d->ny;
+        a.n = d->nxt;
+    } else {
+        a.bnd_lo = d->bnd_down;
+        a.bnd_hi = d->bnd_up;
+        a.nlines = d->nx;
+        a.n = d->nyt;
+    }
+    a.seg = kSeg;
+    return a;
+}
+
+static cudaEvent_t take_event(hb_domain* d) {
+    if (!d->ev_pool.empty()) {
+        cudaEvent_t e = d->ev_pool.back();
+        d->ev_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+static int launch_sweep_timed(hb_domain* d, int dir, const SweepArgs& a) {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (d->prof) {
+        e0 = take_event(d);
+        e1 = take_event(d);
+        HB_CU(cudaEventRecord(e0, d->stream));
+    }
+    HB_CU(hb::launch_sweep(dir, a, d->P, d->stream));
+    d->launches += 1;
+    if (d->prof) {
+        HB_CU(cudaEventRecord(e1, d->stream));
+        d->ev_pending.push_back(e0);
+        d->ev_pending.push_back(e1);
+        d->ev_dir.push_back(dir);
+    }
+    return HB_OK;
+}
+
+// hydro_godunov.c:70-139: first sweep A -> B (ghosts of its direction written
+// to A), second sweep B -> A (ghosts of the second direction written to A).
+// With fuse, the second sweep also reduces the Courant maxima of the result.
+static int domain_step(hb_domain* d, int idim, double dt, const DevClock* clk, bool fuse) {
+    const int first = (idim == 1) ? 1 : 2;
+    const int second = 3 - first;
+    if (fuse) {
+        HB_CU(cudaMemsetAsync(d->cour, 0, 2 * sizeof(unsigned long long), d->stream));
+    }
+    SweepArgs a1 = sweep_args(d, first, d->A, d->B, clk, dt, nullptr);
+    int rc = launch_sweep_timed(d, first, a1);
+    if (rc) return rc;
+    SweepArgs a2 = sweep_args(d, second, d->B, d->A, clk, dt, fuse ? d->cour : nullptr);
+    rc = launch_sweep_timed(d, second, a2);
+    if (rc) return rc;
+    d->cour_valid = fuse;
+    return HB_OK;
+}
+
+extern "C" int hydro_b200_domain_godunov(hb_domain* d, int idim, double dt, int fuse_courant) {
+    if (!d) return set_error(HB_ERR_ARG, "null domain");
+    if (idim != 1 && idim != 2) return set_error(HB_ERR_ARG, "idim=%d: expected 1 or 2", idim);
+    return domain_step(d, idim, dt, nullptr, fuse_courant != 0);
+}
+
+extern "C" int hydro_b200_domain_profile(hb_domain* d, int enable) {
+    if (!d) return set_error(HB_ERR_ARG, "null domain");
+    d->prof = enable != 0;
+    return HB_OK;
+}
+
+// Waits for the recorded sweeps and returns the accumulated time (ms) and
+// launch count of the x (index 0) and y (index 1) sweeps; reset clears them.
+extern "C" int hydro_b200_domain_profile_read(hb_domain* d, double* ms, long long* count,
+                                              int reset) {
+    if (!d) return set_error(HB_ERR_ARG, "null domain");
+    HB_CU(cudaStreamSynchronize(d->stream));
+    for (size_t i = 0; i < d->ev_dir.size(); i++) {
+        float t = 0.f;
+        HB_CU(cudaEventElapsedTime(&t, d->ev_pending[2 * i], d->ev_pending[2 * i + 1]));
+        d->prof_ms[d->ev_dir[i] - 1] += t;
+        d->prof_n[d->ev_dir[i] - 1] += 1;
+    }
+    for (cudaEvent_t e : d->ev_pending) d->ev_pool.push_back(e);
+    d->ev_pending.clear();
+    d->ev_dir.clear();
+    if (ms) {
+        ms[0] = d->prof_ms[0];
+        ms[1] = d->prof_ms[1];
+    }
+    if (count) {
+        count[0] = d->prof_n[0];
+        count[1] = d->prof_n[1];
+    }
+    if (reset) {
+        d->prof_ms[0] = d->prof_ms[1] = 0.0;
+        d->prof_n[0] = d->prof_n[1] = 0;
+    }
+    return HB_OK;
+}
+
+extern "C" int hydro_b200_domain_make_boundary(hb_domain* d, int idim) {
+    if (!d) return set_error(HB_ERR_ARG, "null domain");
+    if (idim != 1 && idim != 2) return set_error(HB_ERR_ARG, "idim=%d: expected 1 or 2", idim);
+    const int lo = idim == 1 ? d->bnd_left : d->bnd_down;
+    const int hi = idim == 1 ? d->bnd_right : d->bnd_up;
+    HB_CU(hb::launch_boundary(d->A, idim, d->nx, d->ny, d->nxt, d->nyt, d->vs, lo, hi,
+                              d->stream));
+    d->launches += 1;
+    return HB_OK;
+}
+
+static int ensure_courant(hb_domain* d) {
+    if (d->cour_valid) return HB_OK;
+    HB_CU(cudaMemsetAsync(d->cour, 0, 2 * sizeof(unsigned long long), d->stream));
+    HB_CU(hb::launch_courant(d->A, d->nx, d->ny, d->nxt, d->vs, d->P, d->cour, d->stream));
+    d->launches += 1;
+    d->cour_valid = true;
+    return HB_OK;
+}
+
+extern "C" int hydro_b200_domain_courant(hb_domain* d, double* cx, double* cy) {
+    if (!d) return set_error(HB_ERR_ARG, "null domain");
+    int rc = ensure_courant(d);
+    if (rc) return rc;
+    unsigned long long h[2];
+    HB_CU(cudaMemcpyAsync(h, d->cour, sizeof(h), cudaMemcpyDeviceToHost, d->stream));
+    HB_CU(cudaStreamSynchronize(d->stream));
+    double x, y;
+    memcpy(&x, &h[0], 8);
+    memcpy(&y, &h[1], 8);
+    if (cx) *cx = x;
+    if (cy) *cy = y;
+    return HB_OK;
+}
+
+extern "C" int hydro_b200_domain_set_clock(hb_domain* d, double t, int nstep, double dt) {
+    if (!d) return set_error(HB_ERR_ARG, "null domain");
+    DevClock c;
+    memset(&c, 0, sizeof(c));
+    c.t = t;
+    c.dt = dt;
+    c.tend = 0.0;
+    c.nstep = nstep;
+    c.nstep0 = nstep;
+    c.nstepmax = nstep;
+    c.active = 1;
+    c.dts = d->dts;
+    c.ndts = d->ndts;
+    HB_CU(cudaMemcpyAsync(d->clk, &c, sizeof(c), cudaMemcpyHostToDevice, d->stream));
+    HB_CU(cudaStreamSynchronize(d->stream));
+    d->h_nstep = nstep;
+    return HB_OK;
+}
+
+// Reserve the device record for the dt of the next n steps.
+static int ensure_dts(hb_domain* d, int n) {
+    if (n <= d->ndts) return HB_OK;
+    cudaFree(d->dts);
+    d->dts = nullptr;
+    d->ndts = 0;
+    HB_CU(cudaMalloc(&d->dts, (size_t)n * sizeof(double)));
+    d->ndts = n;
+    return HB_OK;
+}
+
+// Asynchronous: per step one clock kernel (dt on even steps, stop test), the
+// two sweeps (Courant reduction fused into the second sweep of odd steps) and
+// one clock kernel (t += dt, nstep++).
+extern "C" int hydro_b200_domain_launch_steps(hb_domain* d, int nsteps, int nstepmax,
+                                              double tend) {
+    if (!d) return set_error(HB_ERR_ARG, "null domain");
+    // Update the limits in the device clock (fields tend, nstepmax).
+    HB_CU(cudaMemcpyAsync((char*)d->clk + offsetof(DevClock, tend), &tend, sizeof(double),
+                          cudaMemcpyHostToDevice, d->stream));
+    HB_CU(cudaMemcpyAsync((char*)d->clk + offsetof(DevClock, nstepmax), &nstepmax, sizeof(int),
+                          cudaMemcpyHostToDevice, d->stream));
+    for (int s = 0; s < nsteps; s++) {
+        const int n = d->h_nstep;
+        if (n % 2 == 0) {
+            int rc = ensure_courant(d);
+            if (rc) return rc;
+        }
+        HB_CU(hb::launch_clock_begin(d->clk, d->cour, d->courant_factor, d->P.dx, d->P.smallc,
+                                     d->stream));
+        int rc = domain_step(d, (n % 2 == 0) ? 1 : 2, 0.0, d->clk, (n % 2) == 1);
+        if (rc) return rc;
+        HB_CU(hb::launch_clock_end(d->clk, d->stream));
+        d->launches += 2;
+        d->h_nstep++;
+        // clock_begin of an even step consumed (zeroed) the accumulators.
+        if (n % 2 == 0) d->cour_valid = false;
+    }
+    return HB_OK;
+}
+
+extern "C" int hydro_b200_domain_get_clock(hb_domain* d, double* t, int* nstep, double* dt) {
+    if (!d) return set_error(HB_ERR_ARG, "null domain");
+    DevClock c;
+    HB_CU(cudaMemcpyAsync(&c, d->clk, sizeof(c), cudaMemcpyDeviceToHost, d->stream));
+    HB_CU(cudaStreamSynchronize(d->stream));
+    if (t) *t = c.t;
+    if (nstep) *nstep = c.nstep;
+    if (dt) *dt = c.dt;
+    return HB_OK;
+}
+
+extern "C" int hydro_b200_domain_get_dts(hb_domain* d, double* dts, int n) {
+    if (!d || !dts) return set_error(HB_ERR_ARG, "null argument");
+    if (n > d->ndts) return set_error(HB_ERR_ARG, "only %d dt records reserved", d->ndts);
+    if (n <= 0) return HB_OK;
+    HB_CU(cudaMemcpyAsync(dts, d->dts, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost,
+                          d->stream));
+    HB_CU(cudaStreamSynchronize(d->stream));
+    return HB_OK;
+}
+
+// ------------------------------------------------- mirror registry (ref ABI)
+struct Mirror {
+    hb_domain* dom;
+};
+static std::mutex g_mu;
+static std::unordered_map<const void*, Mirror> g_mirrors;
+
+static bool sync_each_call() {
+    const char* s = getenv("HYDRO_B200_SYNC");
+    return s && s[0] == '1';
+}
+
+// Find (or create and upload) the mirror of Hv->uold for the grid of H.
+static hb_domain* mirror_for(const hydroparam_t* H, hydrovar_t* Hv) {
+    if (!Hv || !Hv->uold) {
+        set_error(HB_ERR_ARG, "null hydrovar_t or uold");
+        return nullptr;
+    }
+    if (validate(H) != HB_OK) return nullptr;
+    std::lock_guard<std::mutex> lk(g_mu);
+    auto it = g_mirrors.find(Hv->uold);
+    if (it != g_mirrors.end()) {
+        hb_domain* d = it->second.dom;
+        if (d->nx == H->nx && d->ny == H->ny) {
+            load_params(d, H);  // H is passed by value on every call: take its constants
+            return d;
+        }
+        hydro_b200_domain_destroy(d);
+        g_mirrors.erase(it);
+    }
+    hb_domain* d = hydro_b200_domain_create(H);
+    if (!d) return nullptr;
+    if (hydro_b200_domain_upload(d, Hv->uold) != HB_OK) {
+        hydro_b200_domain_destroy(d);
+        return nullptr;
+    }
+    g_mirrors[Hv->uold] = Mirror{d};
+    return d;
+}
+
+extern "C" void* hydro_b200_mirror_stream(const hydroparam_t* H, hydrovar_t* Hv) {
+    hb_domain* d = mirror_for(H, Hv);
+    return d ? (void*)d->stream : nullptr;
+}
+
+extern "C" int hydro_b200_sync_to_host(const hydroparam_t* H, hydrovar_t* Hv) {
+    hb_domain* d = mirror_for(H, Hv);
+    if (!d) return g_err;
+    int rc = hydro_b200_domain_download(d, Hv->uold);
+    if (rc) return rc;
+    return hydro_b200_domain_synchronize(d);
+}
+
+extern "C" int hydro_b200_sync_to_device(const hydroparam_t* H, hydrovar_t* Hv) {
+    hb_domain* d = mirror_for(H, Hv);
+    if (!d) return g_err;
+    int rc = hydro_b200_domain_upload(d, Hv->uold);
+    if (rc) return rc;
+    return hydro_b200_domain_synchronize(d);
+}
+
+extern "C" int hydro_b200_release(hydrovar_t* Hv) {
+    if (!Hv) return set_error(HB_ERR_ARG, "null hydrovar_t");
+    std::lock_guard<std::mutex> lk(g_mu);
+    auto it = g_mirrors.find(Hv->uold);
+    if (it == g_mirrors.end()) return HB_OK;
+    hydro_b200_domain_destroy(it->second.dom);
+    g_mirrors.erase(it);
+    return HB_OK;
+}
+
+extern "C" void hydro_godunov(int idim, real_t dt, const hydroparam_t H, hydrovar_t* Hv,
+                              hydrowork_t* Hw, hydrovarwork_t* Hvw) {
+    (void)Hw;
+    (void)Hvw;
+    hb_domain* d = mirror_for(&H, Hv);
+    if (!d) return;
+    if (idim != 1 && idim != 2) {
+        set_error(HB_ERR_ARG, "idim=%d: expected 1 or 2", idim);
+        return;
+    }
+    // The reference driver calls compute_deltat right after every idim == 2
+    // step (main.c:349-399): reduce the Courant maxima inside its second sweep.
+    if (domain_step(d, idim, dt, nullptr, idim == 2) != HB_OK) return;
+    if (sync_each_call()) {
+        if (hydro_b200_domain_download(d, Hv->uold) == HB_OK) hydro_b200_domain_synchronize(d);
+    }
+}
+
+extern "C" void compute_deltat(real_t* dt, const hydroparam_t H, hydrowork_t* Hw, hydrovar_t* Hv,
+                               hydrovarwork_t* Hvw) {
+    (void)Hw;
+    (void)Hvw;
+    if (!dt) {
+        set_error(HB_ERR_ARG, "null dt");
+        return;
+    }
+    hb_domain* d = mirror_for(&H, Hv);
+    if (!d) return;
+    double cx = 0.0, cy = 0.0;
+    if (hydro_b200_domain_courant(d, &cx, &cy) != HB_OK) return;
+    // compute_deltat.c:73 (MAX of utils.h).
+    double m = cy > H.smallc ? cy : H.smallc;
+    m = cx > m ? cx : m;
+    *dt = H.courant_factor * H.dx / m;
+}
+
+extern "C" void make_boundary(int idim, const hydroparam_t H, hydrovar_t* Hv) {
+    hb_domain* d = mirror_for(&H, Hv);
+    if (!d) return;
+    if (hydro_b200_domain_make_boundary(d, idim) != HB_OK) return;
+    if (sync_each_call()) {
+        if (hydro_b200_domain_download(d, Hv->uold) == HB_OK) hydro_b200_domain_synchronize(d);
+    }
+}
+
+extern "C" void compute_deltat_init_mem(const hydroparam_t H, hydrowork_t* Hw,
+                                        hydrovarwork_t* Hvw) {
+    (void)H;
+    if (Hw) memset(Hw, 0, sizeof(*Hw));
+    if (Hvw) memset(Hvw, 0, sizeof(*Hvw));
+}
+
+extern "C" void compute_deltat_clean_mem(const hydroparam_t H, hydrowork_t* Hw,
+                                         hydrovarwork_t* Hvw) {
+    (void)H;
+    (void)Hw;
+    (void)Hvw;
+    std::lock_guard<std::mutex> lk(g_mu);
+    for (auto& kv : g_mirrors) {
+        hb_domain* d = kv.second.dom;
+        cudaMemcpyAsync((void*)kv.first, d->A, d->nelem * sizeof(double), cudaMemcpyDeviceToHost,
+                        d->stream);
+        cudaStreamSynchronize(d->stream);
+        hydro_b200_domain_destroy(d);
+    }
+    g_mirrors.clear();
+}
+
+extern "C" int hydro_b200_run(const hydroparam_t* H, hydrovar_t* Hv, int nstepmax, real_t tend,
+                              real_t* t, int* nstep, real_t* dt, real_t* dts) {
+    if (!t || !nstep || !dt) return set_error(HB_ERR_ARG, "null t/nstep/dt"), -1;
+    hb_domain* d = mirror_for(H, Hv);
+    if (!d) return -1;
+    const int todo = nstepmax - *nstep;
+    if (todo <= 0 || !(*t < tend)) return 0;
+    if (ensure_dts(d, todo) != HB_OK) return -1;
+    if (hydro_b200_domain_set_clock(d, *t, *nstep, *dt) != HB_OK) return -1;
+    if (hydro_b200_domain_launch_steps(d, todo, nstepmax, tend) != HB_OK) return -1;
+    int n1 = *nstep;
+    if (hydro_b200_domain_get_clock(d, t, &n1, dt) != HB_OK) return -1;
+    const int done = n1 - *nstep;
+    if (dts && done > 0 && hydro_b200_domain_get_dts(d, dts, done) != HB_OK) return -1;
+    *nstep = n1;
+    // The host's parity view must follow the device clock when it stopped early.
+    d->h_nstep = n1;
+    d->cour_valid = false;
+    return done;
+}
+
+extern "C" int hydro_b200_set_device(int device) {
+    HB_CU(cudaSetDevice(device));
+    return HB_OK;
+}
+
+extern "C" const char* hydro_b200_build_info(void) {
+    return "hydro_b200: FP64 fused sweeps, sm_100a, --fmad=false, IEEE div/sqrt";
+}

@@ -1,0 +1,281 @@
+// hb_stages.cuh -- per-cell / per-interface device functions of the HydroC
+// Godunov/MUSCL step, FP64.
+//
+// Every function restates the arithmetic of the reference
+// (HydroC/HydroC99_2Domp/Src, cited per function) with the same IEEE
+// operations in the same order.  The translation unit that includes this file
+// is compiled with --fmad=false and IEEE division / square root, so each
+// operation is rounded once, exactly as in the reference's C build (gcc -O3
+// -mavx2, no FMA): the kernels reproduce the reference bit for bit.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace hb {
+
+// Primitive variables of one cell in line orientation: density, velocity
+// normal to the sweep, transverse velocity, pressure.
+struct Prim {
+    double r, u, v, p;
+};
+
+// Conservative variables in line orientation: rho, normal momentum,
+// transverse momentum, total energy.
+struct Cons {
+    double d, mn, mt, e;
+};
+
+// Constants of one run, derived on the host with the reference's formulas.
+struct Phys {
+    double gamma, gm1;    // gamma, gamma - 1 (equation_of_state.c:42)
+    double smallr, smallc;
+    double smallp;        // smallc^2 / gamma (equation_of_state.c:25, riemann.c:34)
+    double gamma6;        // (gamma + 1) / (2 gamma) (riemann.c:35)
+    double smallpp;       // smallr * smallp (riemann.c:36)
+    double entho;         // 1 / (gamma - 1) (cmpflx.c:27)
+    double slope_type;
+    double dx;
+    int niter;            // niter_riemann
+    int iorder;           // 1: first order (dq = 0)
+    int scheme;           // 1 muscl, 2 plmde, 3 collela
+    int unit_slope;       // slope_type == 1.0 (x*1 and x/1 are exact: skipped)
+};
+
+// utils.h:9-11 MAX(x, y): x > y ? x : y.
+__device__ __forceinline__ double omax(double x, double y) { return x > y ? x : y; }
+
+// C99 fmax / fmin as glibc evaluates them: the non-NaN operand if one is NaN,
+// otherwise x when x >= y (resp. x <= y) -- so ties between +0 and -0 return
+// the first operand, which PTX max.f64/min.f64 do not promise.
+__device__ __forceinline__ double cfmax(double x, double y) {
+    return (x >= y || y != y) ? x : y;
+}
+__device__ __forceinline__ double cfmin(double x, double y) {
+    return (x <= y || y != y) ? x : y;
+}
+
+// constoprim.c:37-52 then equation_of_state.c:41-48.
+__device__ __forceinline__ void cons_to_prim(const Phys& P, const Cons& u, Prim& q, double& c) {
+    double r = omax(u.d, P.smallr);
+    double un = u.mn / r;
+    double ut = u.mt / r;
+    double eken = 0.5 * ((un * un) + (ut * ut));
+    double e = u.e / r - eken;
+    double base = P.gm1 * r * e;
+    base = omax(base, r * P.smallp);
+    q.r = r;
+    q.u = un;
+    q.v = ut;
+    q.p = base;
+    c = sqrt(P.gamma * base / r);
+}
+
+// slope.c:37-50 for one variable.
+template <bool UNIT>
+__device__ __forceinline__ double slope1(double st, double qm, double q0, double qp) {
+    double dlft, drgt, dcen;
+    if (UNIT) {
+        dlft = q0 - qm;
+        drgt = qp - q0;
+        dcen = 0.5 * (dlft + drgt);
+    } else {
+        dlft = st * (q0 - qm);
+        drgt = st * (qp - q0);
+        dcen = 0.5 * (dlft + drgt) / st;
+    }
+    double dsgn = (dcen > 0.0) ? 1.0 : -1.0;
+    int llftrgt = ((dlft * drgt) <= 0.0);
+    double t1 = cfmin(fabs(dlft), fabs(drgt));
+    return dsgn * cfmin((double)(1 - llftrgt) * t1, fabs(dcen));
+}
+
+template <bool UNIT>
+__device__ __forceinline__ void slope4(double st, const Prim& a, const Prim& b, const Prim& c,
+                                       Prim& dq) {
+    dq.r = slope1<UNIT>(st, a.r, b.r, c.r);
+    dq.u = slope1<UNIT>(st, a.u, b.u, c.u);
+    dq.v = slope1<UNIT>(st, a.v, b.v, c.v);
+    dq.p = slope1<UNIT>(st, a.p, b.p, c.p);
+}
+
+// Scheme constants of trace.c:30-46.
+struct TraceK {
+    double dtdx, zerol, zeror, project;
+};
+
+__device__ __forceinline__ TraceK trace_constants(int scheme, double dtdx) {
+    TraceK k;
+    k.dtdx = dtdx;
+    k.zerol = 0.0;
+    k.zeror = 0.0;
+    k.project = 0.0;
+    if (scheme == 1) {
+        k.zerol = -100.0 / dtdx;
+        k.zeror = 100.0 / dtdx;
+        k.project = 1.0;
+    }
+    if (scheme == 2) {
+        k.project = 1.0;
+    }
+    return k;
+}
+
+// trace.c:63-123 for one cell: left (qxm) and right (qxp) states.
+__device__ __forceinline__ void trace1(const TraceK& K, const Prim& q, const Prim& dq, double cc,
+                                       Prim& qxm, Prim& qxp) {
+    const double dtdx = K.dtdx;
+    double csq = cc * cc;
+    double rOcc = q.r / cc;
+    double OrOcc = cc / q.r;
+    double dprcc = dq.p / (q.r * cc);
+    double alpham = 0.5 * (dprcc - dq.u) * rOcc;
+    double alphap = 0.5 * (dprcc + dq.u) * rOcc;
+    double alpha0r = dq.r - dq.p / csq;
+    double alpha0v = dq.v;
+    double upcc = q.u + cc;
+    double umcc = q.u - cc;
+    double upccx = upcc * dtdx;
+    double umccx = umcc * dtdx;
+    double ux = q.u * dtdx;
+
+    double spminus = (umcc >= K.zeror) ? (K.project) : umccx + 1.0;
+    double spplus = (upcc >= K.zeror) ? (K.project) : upccx + 1.0;
+    double spzero = (q.u >= K.zeror) ? (K.project) : ux + 1.0;
+    double ap = -0.5 * spplus * alphap;
+    double am = -0.5 * spminus * alpham;
+    double azr = -0.5 * spzero * alpha0r;
+    double azv = -0.5 * spzero * alpha0v;
+    qxp.r = q.r + (ap + am + azr);
+    qxp.u = q.u + (ap - am) * OrOcc;
+    qxp.v = q.v + (azv);
+    qxp.p = q.p + (ap + am) * csq;
+
+    spminus = (umcc <= K.zerol) ? (-K.project) : umccx - 1.0;
+    spplus = (upcc <= K.zerol) ? (-K.project) : upccx - 1.0;
+    spzero = (q.u <= K.zerol) ? (-K.project) : ux - 1.0;
+    ap = -0.5 * spplus * alphap;
+    am = -0.5 * spminus * alpham;
+    azr = -0.5 * spzero * alpha0r;
+    azv = -0.5 * spzero * alpha0v;
+    qxm.r = q.r + (ap + am + azr);
+    qxm.u = q.u + (ap - am) * OrOcc;
+    qxm.v = q.v + (azv);
+    qxm.p = q.p + (ap + am) * csq;
+}
+
+// riemann.c:89-110 (first guess), :126-156 (Newton iterations on p*, at most
+// niter, stopping per interface once |dp/p| <= 1e-6), :175-258 (sampling, with
+// the C99 selection order: outer state if spout < 0, else star state if
+// spin > 0, else the blend), then the flux of the Godunov state
+// (cmpflx.c:52-73).  ql = qxm of the cell left of the interface, qr = qxp of
+// the cell to its right (qleftright.c:45-46).
+__device__ __forceinline__ Cons riemann_flux(const Phys& P, const Prim& ql, const Prim& qr) {
+    const double gamma = P.gamma, smallr = P.smallr, smallc = P.smallc, smallp = P.smallp;
+    const double gamma6 = P.gamma6;
+
+    double rl = cfmax(ql.r, smallr);
+    double ul = ql.u;
+    double pl = cfmax(ql.p, rl * smallp);
+    double rr = cfmax(qr.r, smallr);
+    double ur = qr.u;
+    double pr = cfmax(qr.p, rr * smallp);
+    double cl = gamma * pl * rl;
+    double cr = gamma * pr * rr;
+    double wl = sqrt(cl);
+    double wr = sqrt(cr);
+    double pstar = cfmax(((wr * pl + wl * pr) + wl * wr * (ul - ur)) / (wl + wr), 0.0);
+
+    for (int iter = 0; iter < P.niter; iter++) {
+        double pst = pstar;
+        double wwl = sqrt(cl * (1.0 + gamma6 * (pst - pl) / pl));
+        double wwr = sqrt(cr * (1.0 + gamma6 * (pst - pr) / pr));
+        double swwl = wwl * wwl;
+        double qlw = 2.0 * wwl * swwl / (swwl + cl);
+        double qrw = 2.0 * wwr * (wwr * wwr) / ((wwr * wwr) + cr);
+        double usl = ul - (pst - pl) / wwl;
+        double usr = ur + (pst - pr) / wwr;
+        double tmp = (qrw * qlw / (qrw + qlw) * (usl - usr));
+        double delp = omax(tmp, (-pst));
+        pst += delp;
+        double tmp2 = delp / (pst + P.smallpp);
+        double conv = fabs(tmp2);
+        pstar = pst;
+        if (!(conv > 1e-6)) break;
+    }
+
+    wr = sqrt(cr * (1.0 + gamma6 * (pstar - pr) / pr));
+    wl = sqrt(cl * (1.0 + gamma6 * (pstar - pl) / pl));
+    double ustar = 0.5 * (ul + (pl - pstar) / wl + ur - (pr - pstar) / wr);
+    bool left = ustar > 0.0;
+    double sgnm = left ? 1.0 : -1.0;
+    double ro = left ? rl : rr;
+    double uo = left ? ul : ur;
+    double po = left ? pl : pr;
+    double wo = left ? wl : wr;
+    double co = sqrt(fabs(gamma * po / ro));
+    co = cfmax(smallc, co);
+    double rstar = ro / (1.0 + ro * (po - pstar) / (wo * wo));
+    rstar = cfmax(rstar, smallr);
+    double cstar = sqrt(fabs(gamma * pstar / rstar));
+    cstar = cfmax(smallc, cstar);
+    double spout = co - sgnm * uo;
+    double spin = cstar - sgnm * ustar;
+    double ushock = wo / ro - sgnm * uo;
+    if (pstar >= po) {
+        spin = ushock;
+        spout = ushock;
+    }
+    double scr = cfmax(spout - spin, smallc + fabs(spout + spin));
+    double frac = (1.0 + (spout + spin) / scr) * 0.5;
+    frac = cfmax(0.0, cfmin(1.0, frac));
+    double gr, gu, gp;
+    if (spout < 0.0) {
+        gr = ro;
+        gu = uo;
+        gp = po;
+    } else if (spin > 0.0) {
+        gr = rstar;
+        gu = ustar;
+        gp = pstar;
+    } else {
+        gr = (frac * rstar + (1.0 - frac) * ro);
+        gu = (frac * ustar + (1.0 - frac) * uo);
+        gp = (frac * pstar + (1.0 - frac) * po);
+    }
+    double gv = left ? ql.v : qr.v;
+
+    Cons f;
+    double mass = gr * gu;
+    f.d = mass;
+    f.mn = mass * gu + gp;
+    f.mt = mass * gv;
+    double ekin = 0.5 * gr * ((gu * gu) + (gv * gv));
+    double etot = gp * P.entho + ekin;
+    f.e = gu * (etot + gp);
+    return f;
+}
+
+// conservar.c:166-172: u + (F_left - F_right) * dtdx, difference first.
+__device__ __forceinline__ Cons update(const Cons& u, const Cons& fl, const Cons& fr, double dtdx) {
+    Cons o;
+    o.d = u.d + (fl.d - fr.d) * dtdx;
+    o.mn = u.mn + (fl.mn - fr.mn) * dtdx;
+    o.mt = u.mt + (fl.mt - fr.mt) * dtdx;
+    o.e = u.e + (fl.e - fr.e) * dtdx;
+    return o;
+}
+
+// Courant speeds of one updated cell: ComputeQEforRow.c:31-47,
+// equation_of_state.c:41-48, courantOnXY.c:44-45.  cn / ct: c + |u| along the
+// sweep's normal / transverse direction.
+__device__ __forceinline__ void courant_speeds(const Phys& P, const Cons& u, double& cn,
+                                               double& ct) {
+    Prim q;
+    double c;
+    cons_to_prim(P, u, q, c);
+    cn = c + fabs(q.u);
+    ct = c + fabs(q.v);
+}
+
+}  // namespace hb

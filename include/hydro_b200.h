@@ -1,0 +1,205 @@
+/*
+ * hydro_b200.h -- C ABI of libhydro_b200.so, the B200 (sm_100a) implementation
+ * of HydroC's dimensionally split Godunov/MUSCL time step.
+ *
+ * Two groups of entry points:
+ *
+ * 1. The reference's own hot-path entry points, with the exact signatures of
+ *    HydroC/HydroC99_2Domp/Src (real_t = double).  A program built against the
+ *    reference links this library in place of hydro_godunov.c and the files
+ *    the reference Makefile lists as offloadable (SRC2, Makefile:118-119).
+ *    The state Hv->uold stays host memory owned by the caller; the library
+ *    keeps a device-resident mirror keyed by that pointer (uploaded on first
+ *    use, copied back by hydro_b200_sync_to_host or, with the environment
+ *    variable HYDRO_B200_SYNC=1, after every hydro_godunov call).
+ *    Hw / Hvw (the reference's host work arrays) are accepted and ignored.
+ *
+ * 2. hydro_b200_* extensions: explicit residency control, a device-resident
+ *    multi-step driver, error reporting and a device-pointer level API.
+ *
+ * The reference functions return void and abort on failure.  Here they record
+ * a thread-local error (hydro_b200_last_error) and return; with
+ * HYDRO_B200_STRICT=1 in the environment they print the error and abort().
+ * All entry points are meant to be called from one host thread.
+ */
+#ifndef HYDRO_B200_H
+#define HYDRO_B200_H
+
+#include <stddef.h>
+#include <stdio.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------
+ * Types.  When the reference's parametres.h was included first (its guard
+ * PARAMETRES_H_INCLUDED is defined) its definitions are used; otherwise these
+ * layout-identical ones are (parametres.h:31-122; the layout is checked field
+ * by field against the reference in tests/test_abi.py).
+ * ------------------------------------------------------------------------ */
+#ifndef PARAMETRES_H_INCLUDED
+typedef double real_t;
+
+enum { HB_XMIN_BOX, HB_XMAX_BOX, HB_YMIN_BOX, HB_YMAX_BOX, HB_UP_BOX, HB_DOWN_BOX,
+       HB_LEFT_BOX, HB_RIGHT_BOX, HB_MAX_BOX };
+
+typedef struct _hydroparam {
+    int prt;
+    real_t t, tend;
+    int nstep, nstepmax;
+    int noutput;
+    real_t dtoutput;
+    int nimage;
+    real_t dtimage;
+    int imin, imax, jmin, jmax, nx, ny, nxt, nyt, nxyt, nxystep;
+    int nproc, mype;
+    int globnx, globny;
+    int box[HB_MAX_BOX];
+    int nvar;
+    real_t dx;
+    real_t gamma;
+    real_t courant_factor;
+    real_t smallc, smallr;
+    int niter_riemann;
+    int iorder;
+    real_t slope_type;
+    int scheme;
+    int boundary_right, boundary_left, boundary_down, boundary_up;
+    int testCase;
+    int shrinkSize;
+    int shrink;
+    FILE *fp;
+} hydroparam_t;
+
+#define HSCHEME_MUSCL 1
+#define HSCHEME_PLMDE 2
+#define HSCHEME_COLLELA 3
+
+typedef struct _hydrovar {
+    real_t *uold; /* [nvar][nyt][nxt], index i + nxt*(j + nyt*v) */
+} hydrovar_t;
+
+typedef struct _hydrovarwork {
+    real_t *u, *q, *qxm, *qxp, *dq;
+    real_t *qleft, *qright, *qgdnv, *flux;
+} hydrovarwork_t;
+
+typedef struct _hydrowork {
+    real_t *c;
+    real_t *e;
+    real_t *tmpm1, *tmpm2;
+    real_t *rl, *ul, *pl, *cl, *wl;
+    real_t *rr, *ur, *pr, *cr, *wr;
+    real_t *ro, *uo, *po, *co, *wo;
+    real_t *rstar, *ustar, *pstar, *cstar;
+    real_t *spin, *spout, *ushock;
+    int *sgnm;
+    int *goon;
+    real_t *frac, *scr, *delp, *pold;
+    int *ind, *ind2;
+} hydrowork_t;
+#endif /* PARAMETRES_H_INCLUDED */
+
+/* ------------------------------------------------------------------------
+ * 1. Reference entry points (drop-in).
+ * ------------------------------------------------------------------------ */
+
+/* Replaces hydro_godunov.c:26-145 (declared hydro_godunov.h:4-5): two sweeps,
+ * x then y for idim == 1, y then x for idim == 2, each one fused kernel
+ * (ghost fill, gather, constoprim, equation_of_state, slope, trace,
+ * qleftright, riemann, cmpflx, update).  With idim == 2 the Courant maxima of
+ * the resulting state are reduced inside the second sweep and cached for the
+ * next compute_deltat. */
+void hydro_godunov(int idim, real_t dt, const hydroparam_t H, hydrovar_t *Hv, hydrowork_t *Hw,
+                   hydrovarwork_t *Hvw);
+
+/* Replaces compute_deltat.c:31-77 (declared compute_deltat.h:10-11):
+ * *dt = courant_factor*dx / max(max|c+u|, max|c+v|, smallc) over the interior. */
+void compute_deltat(real_t *dt, const hydroparam_t H, hydrowork_t *Hw, hydrovar_t *Hv,
+                    hydrovarwork_t *Hvw);
+
+/* Replaces make_boundary.c:21-206 (declared make_boundary.h:6): fills the two
+ * ghost layers of direction idim on the device mirror. */
+void make_boundary(int idim, const hydroparam_t H, hydrovar_t *Hv);
+
+/* Replace compute_deltat.c:15-29 (declared compute_deltat.h:7-8).  init_mem
+ * allocates nothing (the device path needs no host work arrays) and sets the
+ * pointers to NULL; clean_mem copies every device mirror back to its host
+ * array and releases it (the reference driver calls it once, after the time
+ * loop: main.c:500). */
+void compute_deltat_init_mem(const hydroparam_t H, hydrowork_t *Hw, hydrovarwork_t *Hvw);
+void compute_deltat_clean_mem(const hydroparam_t H, hydrowork_t *Hw, hydrovarwork_t *Hvw);
+
+/* ------------------------------------------------------------------------
+ * 2. Extensions.
+ * ------------------------------------------------------------------------ */
+
+/* Error codes. */
+#define HB_OK 0
+#define HB_ERR_ARG 1        /* invalid argument / unsupported parameter set */
+#define HB_ERR_CUDA 2       /* a CUDA runtime call failed */
+#define HB_ERR_NODEV 3      /* no CUDA device */
+#define HB_ERR_NOMEM 4      /* device allocation failed */
+#define HB_ERR_STATE 5      /* non-finite or non-positive density detected */
+#define HB_ERR_TIMEOUT 6    /* a bounded device-side wait gave up */
+
+int hydro_b200_last_error(void);
+const char *hydro_b200_last_error_message(void);
+void hydro_b200_clear_error(void);
+
+/* Residency of the mirror keyed by Hv->uold. */
+int hydro_b200_sync_to_host(const hydroparam_t *H, hydrovar_t *Hv);   /* device -> host */
+int hydro_b200_sync_to_device(const hydroparam_t *H, hydrovar_t *Hv); /* host -> device */
+int hydro_b200_release(hydrovar_t *Hv); /* frees the mirror (no copy back) */
+/* Stream (a cudaStream_t) on which the mirror of Hv->uold runs; creates and
+ * uploads the mirror if needed. */
+void *hydro_b200_mirror_stream(const hydroparam_t *H, hydrovar_t *Hv);
+
+/* Device-resident driver loop with the semantics of main.c:344-408: from
+ * (*t, *nstep, *dt) run until t >= tend or nstep >= nstepmax, recomputing dt
+ * on even steps (halved at step 0), x->y sweeps on even steps and y->x on odd
+ * steps, with dt and t kept on the device (no host synchronisation inside
+ * the loop).  dts (optional, nstepmax - *nstep entries) receives the dt of each
+ * step.  Returns the number of steps done, or -1 on error. */
+int hydro_b200_run(const hydroparam_t *H, hydrovar_t *Hv, int nstepmax, real_t tend, real_t *t,
+                   int *nstep, real_t *dt, real_t *dts);
+
+/* Device-pointer level API (no host state involved).  A "domain" owns a
+ * device state in the reference layout plus its scratch buffer, stream and
+ * device clock.  The stream is returned as a void* (a cudaStream_t). */
+typedef struct hb_domain hb_domain;
+hb_domain *hydro_b200_domain_create(const hydroparam_t *H);
+void hydro_b200_domain_destroy(hb_domain *d);
+double *hydro_b200_domain_state(hb_domain *d); /* device pointer, 4*nxt*nyt doubles */
+void *hydro_b200_domain_stream(hb_domain *d);
+int hydro_b200_domain_upload(hb_domain *d, const double *host);    /* async on the stream */
+int hydro_b200_domain_download(hb_domain *d, double *host);        /* async on the stream */
+int hydro_b200_domain_synchronize(hb_domain *d);
+int hydro_b200_domain_godunov(hb_domain *d, int idim, double dt, int fuse_courant);
+int hydro_b200_domain_make_boundary(hb_domain *d, int idim);
+int hydro_b200_domain_courant(hb_domain *d, double *cournox, double *cournoy); /* synchronous */
+/* Launch-only driver (asynchronous; same semantics as hydro_b200_run). */
+int hydro_b200_domain_set_clock(hb_domain *d, double t, int nstep, double dt);
+int hydro_b200_domain_launch_steps(hb_domain *d, int nsteps, int nstepmax, double tend);
+int hydro_b200_domain_get_clock(hb_domain *d, double *t, int *nstep, double *dt); /* synchronous */
+int hydro_b200_domain_get_dts(hb_domain *d, double *dts, int n); /* dt of the steps since set_clock */
+/* Event timing of every sweep launch: enable, then read the accumulated
+ * milliseconds and launch counts of x (index 0) and y (index 1) sweeps. */
+int hydro_b200_domain_profile(hb_domain *d, int enable);
+int hydro_b200_domain_profile_read(hb_domain *d, double *ms, long long *count, int reset);
+/* Number of kernel launches the library issued on this domain so far. */
+long long hydro_b200_domain_launch_count(hb_domain *d);
+
+/* Select the CUDA device used by the calling thread for domains and mirrors
+ * created afterwards (the library links its own CUDA runtime, so a device
+ * chosen through another runtime instance does not carry over). */
+int hydro_b200_set_device(int device);
+
+/* Library build information (static string). */
+const char *hydro_b200_build_info(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HYDRO_B200_H */

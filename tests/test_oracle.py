@@ -1,0 +1,106 @@
+"""The CPU restatement (oracle/hydro_oracle.c) pinned against the reference:
+against the golden fixtures made from the reference's own code
+(tests/golden/make_golden.py) and, where the reference was compiled here
+(oracle/_ref), against the reference run side by side."""
+import hashlib
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+from _helpers import bitwise_equal, describe_mismatch
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+CASE_EXTRA = {
+    "reflect_centre_32x24": {},
+    "absorb_corner_29x35": {},
+    "periodic_centre_31x27": {},
+    "mixed_sod_24x24_plmde": {"scheme": 2},
+    "collela_first_order_30x30": {"scheme": 3, "iorder": 1},
+    "slope_half_niter3_28x20": {"slope_type": 0.5, "niter_riemann": 3},
+    "open_sides_26x22": {},
+}
+
+
+def _golden_runs():
+    z = np.load(os.path.join(GOLDEN, "ref_runs.npz"))
+    names = sorted({k.split("__")[0] for k in z.files})
+    return z, names
+
+
+@pytest.mark.parametrize("name", sorted(CASE_EXTRA))
+def test_restatement_matches_reference_golden(oracle, name):
+    z, names = _golden_runs()
+    assert name in names
+    nx, ny, tc, nsteps, *bnd = [int(v) for v in z[f"{name}__meta"]]
+    p = oracle.make_param(nx, ny, boundary=tuple(bnd), **CASE_EXTRA[name])
+    u = oracle.init_state(p, tc)
+    assert bitwise_equal(u, z[f"{name}__init"]), "initial state (hydro_funcs.c:15-112)"
+    n, dts, _ = oracle.run(p, u, nsteps)
+    assert n == nsteps
+    assert bitwise_equal(dts, z[f"{name}__dts"]), "dt sequence"
+    ref = z[f"{name}__final"]
+    assert bitwise_equal(u, ref), describe_mismatch(u, ref)
+
+
+def test_restatement_matches_reference_c0_golden(oracle):
+    with open(os.path.join(GOLDEN, "ref_c0.json")) as f:
+        g = json.load(f)
+    p = oracle.make_param(g["nx"], g["ny"], boundary=(1, 1, 1, 1))
+    assert p.dx == g["dx"]
+    u = oracle.init_state(p, g["testcase"])
+    n, dts, t = oracle.run(p, u, g["nsteps"])
+    assert [float(x).hex() for x in dts] == g["dts"]
+    assert hashlib.sha256(u.tobytes()).hexdigest() == g["sha256"]
+    assert [math.fsum(u[v].ravel().tolist()).hex() for v in range(4)] == g["sums"]
+
+
+def test_restatement_is_thread_count_independent(oracle):
+    p = oracle.make_param(60, 44, boundary=(1, 1, 1, 1))
+    a = oracle.init_state(p, 0)
+    b = a.copy()
+    oracle.run(p, a, 20, threads=1)
+    oracle.run(p, b, 20, threads=4)
+    assert bitwise_equal(a, b)
+
+
+ref_needed = pytest.mark.skipif(
+    not __import__("oracle.oracle", fromlist=["x"]).ref_available(),
+    reason="reference not compiled here (oracle/_ref)")
+
+
+@ref_needed
+@pytest.mark.parametrize("case", [
+    (250, 125, 1, 100, (1, 1, 1, 1), {}),
+    (61, 47, 0, 40, (2, 1, 3, 2), {"scheme": 2}),
+    (40, 64, 2, 30, (3, 3, 1, 1), {"slope_type": 1.7, "niter_riemann": 2}),
+])
+def test_restatement_matches_reference_live(oracle, case):
+    nx, ny, tc, nsteps, bnd, extra = case
+    p = oracle.make_param(nx, ny, boundary=bnd, **extra)
+    r = oracle.RefState(p, tc, nxystep=7)
+    u = oracle.init_state(p, tc)
+    n, dts, _ = oracle.run(p, u, nsteps)
+    n2, dts2, _, _, _ = r.run(nsteps)
+    ur = r.get()
+    r.close()
+    assert n == n2 and bitwise_equal(dts, dts2)
+    assert bitwise_equal(u, ur), describe_mismatch(u, ur)
+
+
+@ref_needed
+def test_make_boundary_matches_reference_live(oracle):
+    rng = np.random.default_rng(5)
+    for bnd in [(1, 1, 1, 1), (2, 2, 2, 2), (3, 3, 3, 3), (0, 2, 1, 0)]:
+        p = oracle.make_param(23, 19, boundary=bnd)
+        r = oracle.RefState(p, 0)
+        u = rng.standard_normal(oracle.state_shape(p))
+        r.set(u)
+        for idim in (1, 2):
+            oracle.make_boundary(p, idim, u)
+            r.make_boundary(idim)
+            assert bitwise_equal(u, r.get()), (bnd, idim)
+        r.close()
