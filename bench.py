@@ -43,6 +43,10 @@ WORKLOADS = {
                run_steps=200),
     "c0": dict(name="hydroc_250x125_corner_blast_fp64", nx=250, ny=125, testcase=1,
                run_steps=100),
+    # The same problem at 2048^2 (134 MB per state buffer, still > L2): the
+    # size the ncu section captures use.
+    "c1_2048": dict(name="hydroc_2048x2048_centre_blast_fp64", nx=2048, ny=2048, testcase=0,
+                    run_steps=200),
 }
 BYTES_PER_CELL_SWEEP = 64   # 4 doubles read + 4 doubles written per cell and sweep
 BYTES_PER_CELL_STEP = 2 * BYTES_PER_CELL_SWEEP

@@ -66,18 +66,17 @@ __device__ __forceinline__ int ghost_source(int bt, int k, int n) {
 }
 
 template <int DIR>
+__device__ __forceinline__ Cons load_interior(const SweepArgs& a, const LineGeom<DIR>& g, int k) {
+    constexpr int mn = Slots<DIR>::mn, mt = Slots<DIR>::mt;
+    const double* __restrict__ p = a.in + g.at(k);
+    return Cons{__ldg(p), __ldg(p + mn * a.vs), __ldg(p + mt * a.vs), __ldg(p + 3 * a.vs)};
+}
+
+template <int DIR>
 __device__ __forceinline__ Cons load_cell(const SweepArgs& a, const LineGeom<DIR>& g, int k) {
     constexpr int mn = Slots<DIR>::mn, mt = Slots<DIR>::mt;
     const long long vs = a.vs;
-    Cons u;
-    if (k >= 2 && k < a.n - 2) {
-        const double* __restrict__ p = a.in + g.at(k);
-        u.d = __ldg(p);
-        u.mn = __ldg(p + mn * vs);
-        u.mt = __ldg(p + mt * vs);
-        u.e = __ldg(p + 3 * vs);
-        return u;
-    }
+    if (k >= 2 && k < a.n - 2) return load_interior<DIR>(a, g, k);
     // Ghost cell: the fused make_boundary.
     const int bt = (k < 2) ? a.bnd_lo : a.bnd_hi;
     const int src = ghost_source<DIR>(bt, k, a.n);
@@ -95,11 +94,7 @@ __device__ __forceinline__ Cons load_cell(const SweepArgs& a, const LineGeom<DIR
             for (int s = 0; s < 4; s++) q[s * vs] = v[s];
         }
     }
-    u.d = v[0];
-    u.mn = v[mn];
-    u.mt = v[mt];
-    u.e = v[3];
-    return u;
+    return Cons{v[0], v[mn], v[mt], v[3]};
 }
 
 template <int DIR>
@@ -136,12 +131,10 @@ sweep_kernel(const SweepArgs a, const Phys P) {
         const int k0 = 2 + blockIdx.y * a.seg;
         const int k1 = min(k0 + a.seg, a.n - 2);
 
-        Cons u1, u2;        // cells k-1, k-2
         Prim q1, q2;        // primitives of k-1, k-2
         double c1 = 0.0;    // sound speed of k-1
         Prim xm2;           // qxm of k-2
         Cons fprev;         // flux at (k-3 | k-2)
-        u1 = u2 = Cons{0.0, 0.0, 0.0, 0.0};
         q1 = q2 = xm2 = Prim{0.0, 0.0, 0.0, 0.0};
         fprev = Cons{0.0, 0.0, 0.0, 0.0};
 
@@ -160,6 +153,9 @@ sweep_kernel(const SweepArgs a, const Phys P) {
                 if (k >= k0 + 1) {
                     f = riemann_flux(P, xm2, xp1);
                     if (k >= k0 + 2) {
+                        // Cell k-2 is interior: its conservative values are read
+                        // again (an L1/L2 hit) instead of being carried.
+                        const Cons u2 = load_interior<DIR>(a, g, k - 2);
                         const Cons o = update(u2, fprev, f, dtdx);
                         store_cell<DIR>(a, g, k - 2, o);
                         if (a.courant) {
@@ -176,8 +172,6 @@ sweep_kernel(const SweepArgs a, const Phys P) {
                     }
                 }
             }
-            u2 = u1;
-            u1 = uk;
             q2 = q1;
             q1 = qk;
             c1 = ck;
@@ -225,6 +219,22 @@ courant_kernel(const double* __restrict__ u, int nx, int ny, int nxt, long long 
     }
     warp_max_atomic(&cour[0], cx);
     warp_max_atomic(&cour[1], cy);
+}
+
+int sweep_blocks_per_sm(int dir, bool unit_slope) {
+    int n = 0;
+    cudaError_t e;
+    if (dir == 1)
+        e = unit_slope ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sweep_kernel<1, true>,
+                                                                       kSweepThreads, 0)
+                       : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sweep_kernel<1, false>,
+                                                                       kSweepThreads, 0);
+    else
+        e = unit_slope ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sweep_kernel<2, true>,
+                                                                       kSweepThreads, 0)
+                       : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, sweep_kernel<2, false>,
+                                                                       kSweepThreads, 0);
+    return (e == cudaSuccess && n > 0) ? n : 1;
 }
 
 cudaError_t launch_courant(const double* u, int nx, int ny, int nxt, long long vs, const Phys& P,

@@ -37,10 +37,12 @@ struct SweepArgs {
     int n;                   // cells along a line including ghosts (nxt or nyt)
 };
 
-constexpr int kSweepThreads = 128;
+constexpr int kSweepThreads = 64;
 
 // Launchers (hb_kernels.cu).  Each returns the cudaError_t of the launch.
 cudaError_t launch_sweep(int dir, const SweepArgs& a, const Phys& P, cudaStream_t s);
+// Resident sweep CTAs per SM (cudaOccupancyMaxActiveBlocksPerMultiprocessor).
+int sweep_blocks_per_sm(int dir, bool unit_slope);
 cudaError_t launch_courant(const double* u, int nx, int ny, int nxt, long long vs, const Phys& P,
                            unsigned long long* cour, cudaStream_t s);
 cudaError_t launch_boundary(double* u, int idim, int nx, int ny, int nxt, int nyt, long long vs,

@@ -80,6 +80,8 @@ struct hb_domain {
     Phys P{};
     double courant_factor = 0.0;
     int bnd_left = 1, bnd_right = 1, bnd_down = 1, bnd_up = 1;
+    int sm_count = 148;
+    int seg[3] = {0, 64, 64};  // output cells per thread segment, per sweep direction
     bool cour_valid = false;  // cour holds the maxima of the current state
     int h_nstep = 0;          // host view of the clock's nstep (parity of launches)
     long long launches = 0;
@@ -149,11 +151,42 @@ extern "C" void hydro_b200_domain_destroy(hb_domain* d) {
     delete d;
 }
 
+// Segment length of a sweep: the grid has ceil(nlines/64) x ceil(nl/seg) CTAs.
+// Pick seg so that the CTA count fills whole waves of the resident slots (no
+// partly filled last wave), while keeping seg >= 24: a segment recomputes a
+// 4-cell halo, about 1.6/seg of the work.
+static int choose_seg(int nlines, int nl, int slots) {
+    const int groups = (nlines + hb::kSweepThreads - 1) / hb::kSweepThreads;
+    int best = 64;
+    double best_score = -1.0;
+    for (int w = 1; w <= 64; w++) {
+        const int nseg_want = (int)((long long)w * slots / groups);
+        if (nseg_want < 1) continue;
+        const int seg = (nl + nseg_want - 1) / nseg_want;
+        if (seg < 24) break;
+        const int nseg = (nl + seg - 1) / seg;
+        const long long ctas = (long long)groups * nseg;
+        const long long waves = (ctas + slots - 1) / slots;
+        const double fill = (double)ctas / (double)(waves * slots);
+        const double score = fill / (1.0 + 1.6 / seg);
+        if (score > best_score + 1e-9) {
+            best_score = score;
+            best = seg;
+        }
+    }
+    return best;
+}
+
 static int domain_alloc(hb_domain* d) {
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
         return set_error(HB_ERR_NODEV, "no CUDA device visible");
     HB_CU(cudaGetDevice(&d->device));
+    HB_CU(cudaDeviceGetAttribute(&d->sm_count, cudaDevAttrMultiProcessorCount, d->device));
+    for (int dir = 1; dir <= 2; dir++) {
+        const int slots = d->sm_count * hb::sweep_blocks_per_sm(dir, d->P.unit_slope != 0);
+        d->seg[dir] = dir == 1 ? choose_seg(d->ny, d->nx, slots) : choose_seg(d->nx, d->ny, slots);
+    }
     HB_CU(cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking));
     HB_CU(cudaMalloc(&d->A, d->nelem * sizeof(double)));
     HB_CU(cudaMalloc(&d->B, d->nelem * sizeof(double)));
@@ -206,8 +239,6 @@ extern "C" int hydro_b200_domain_synchronize(hb_domain* d) {
     return HB_OK;
 }
 
-// Fixed output-cell count per thread segment of the sweeps.
-static constexpr int kSeg = 64;
 
 static SweepArgs sweep_args(hb_domain* d, int dir, const double* in, double* out,
                             const DevClock* clk, double dt, unsigned long long* cour) {
@@ -235,7 +266,7 @@ static SweepArgs sweep_args(hb_domain* d, int dir, const double* in, double* out
         a.nlines = d->nx;
         a.n = d->nyt;
     }
-    a.seg = kSeg;
+    a.seg = d->seg[dir];
     return a;
 }
 

@@ -45,15 +45,12 @@ struct Phys {
 // utils.h:9-11 MAX(x, y): x > y ? x : y.
 __device__ __forceinline__ double omax(double x, double y) { return x > y ? x : y; }
 
-// C99 fmax / fmin as glibc evaluates them: the non-NaN operand if one is NaN,
-// otherwise x when x >= y (resp. x <= y) -- so ties between +0 and -0 return
-// the first operand, which PTX max.f64/min.f64 do not promise.
-__device__ __forceinline__ double cfmax(double x, double y) {
-    return (x >= y || y != y) ? x : y;
-}
-__device__ __forceinline__ double cfmin(double x, double y) {
-    return (x <= y || y != y) ? x : y;
-}
+// C99 fmax / fmin as glibc evaluates them for non-NaN operands: x when
+// x >= y (resp. x <= y), so a tie between +0 and -0 returns the first operand,
+// which PTX max.f64/min.f64 do not promise.  (NaN operands, which a valid
+// state never produces, are not given C99's "return the other operand" rule.)
+__device__ __forceinline__ double cfmax(double x, double y) { return x >= y ? x : y; }
+__device__ __forceinline__ double cfmin(double x, double y) { return x <= y ? x : y; }
 
 // constoprim.c:37-52 then equation_of_state.c:41-48.
 __device__ __forceinline__ void cons_to_prim(const Phys& P, const Cons& u, Prim& q, double& c) {
