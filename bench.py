@@ -166,6 +166,17 @@ def barrier(pg, device):
         pg.all_reduce(torch.zeros(1, device=device))
 
 
+def dom_state_after(H, u0, nsteps, precision):
+    from hydro_b200 import Domain
+    d = Domain(H, precision=precision)
+    d.upload(u0)
+    d.set_clock()
+    d.launch_steps(nsteps)
+    u = d.download()
+    d.close()
+    return u
+
+
 def cpu_reference_sample(wl, budget_s, max_steps, warm=1):
     """The reference's own C99/OpenMP code (oracle/_ref) on the host cores,
     falling back to the C restatement (oracle/_build) where the reference was
@@ -232,6 +243,7 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c1")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
     if args.warmup < 3:
@@ -305,6 +317,37 @@ def main():
     peak, peak_kind = measured_peak_hbm()
     dom.close()
 
+    # The mixed-precision form on the same workload and steps, with its error
+    # against the FP64 state.
+    forms = {}
+    if not args.no_mixed:
+        from hydro_b200.metrics import field_errors
+        ref_state = dom_state_after(H, u0, K, "fp64")
+        dm = Domain(H, precision="mixed")
+        dm.upload(u0)
+        dm.set_clock()
+        dm.launch_steps(W)
+        dm.synchronize()
+        dm.upload(u0)
+        dm.set_clock()
+        sm = torch.cuda.ExternalStream(dm.stream_ptr, device=device)
+        barrier(pg, device)
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record(sm)
+        dm.launch_steps(K)
+        g1.record(sm)
+        g1.synchronize()
+        mix_ms = all_max(pg, g0.elapsed_time(g1), device)
+        mix_state = dm.download()
+        dm.close()
+        err = field_errors(mix_state, ref_state)
+        forms["mixed"] = {"value": round(world * nx * ny * K / (mix_ms / 1e3) / 1e6, 3),
+                          "unit": "Mcell-updates/s", "ms_per_step": round(mix_ms / K, 4),
+                          "speedup_vs_fp64": round(ms_max / mix_ms, 3),
+                          "errors_vs_fp64": err,
+                          "precision": "FP32 stages; FP64 Newton p*, update, Courant"}
+        del ref_state, mix_state
+
     # End to end through the reference entry points on a pinned host array.
     e2e = None
     if not args.no_e2e:
@@ -361,6 +404,7 @@ def main():
         "clocks": clocks,
         "e2e": e2e,
         "cpu_baseline": cpu,
+        "forms": forms,
     }
     print(json.dumps(line), flush=True)
     return 0

@@ -18,6 +18,8 @@ LIB_PATH = os.path.join(PKG_DIR, "libhydro_b200.so")
 MAX_BOX = 8
 
 HB_OK, HB_ERR_ARG, HB_ERR_CUDA, HB_ERR_NODEV, HB_ERR_NOMEM, HB_ERR_STATE, HB_ERR_TIMEOUT = range(7)
+HB_PREC_FP64, HB_PREC_MIXED = 0, 1
+PRECISIONS = {"fp64": HB_PREC_FP64, "mixed": HB_PREC_MIXED}
 
 
 class HydroParam(C.Structure):
@@ -122,6 +124,7 @@ SIGNATURES = [
     ("hydro_b200_domain_get_clock", C.c_int, [_D, _DP, C.POINTER(C.c_int), _DP]),
     ("hydro_b200_domain_get_dts", C.c_int, [_D, _DP, C.c_int]),
     ("hydro_b200_domain_launch_count", C.c_longlong, [_D]),
+    ("hydro_b200_domain_set_precision", C.c_int, [_D, C.c_int]),
     ("hydro_b200_domain_profile", C.c_int, [_D, C.c_int]),
     ("hydro_b200_domain_profile_read", C.c_int, [_D, _DP, C.POINTER(C.c_longlong), C.c_int]),
     ("hydro_b200_set_device", C.c_int, [C.c_int]),

@@ -23,166 +23,14 @@
 // reference's in-place update; the host alternates the buffers so the state
 // ends in the resident array after both sweeps.
 #include "hb_kernels.cuh"
+#include "hb_march.cuh"
 
 namespace hb {
-
-template <int DIR>
-struct LineGeom {
-    // DIR 1: line = row j = l + 2, cells along x.  DIR 2: line = column i = l + 2.
-    long long base;   // offset of cell k = 0 of the line, variable 0
-    long long step;   // offset between consecutive cells of the line
-    __device__ __forceinline__ LineGeom(const SweepArgs& a, int l) {
-        if (DIR == 1) {
-            base = (long long)a.nxt * (l + 2);
-            step = 1;
-        } else {
-            base = l + 2;
-            step = a.nxt;
-        }
-    }
-    __device__ __forceinline__ long long at(int k) const { return base + step * k; }
-};
-
-// Slots of the normal and transverse momentum: IU/IV for x, IV/IU for y
-// (the swap of conservar.c:97-100 and :215-222).
-template <int DIR> struct Slots;
-template <> struct Slots<1> { static constexpr int mn = 1, mt = 2; };
-template <> struct Slots<2> { static constexpr int mn = 2, mt = 1; };
-
-// Ghost source of make_boundary.c:53-198 for position k of a line of n cells
-// (nl = n - 4 interior cells).  Returns -1 when the side has no boundary fill.
-template <int DIR>
-__device__ __forceinline__ int ghost_source(int bt, int k, int n) {
-    const int nl = n - 4;
-    if (bt <= 0) return -1;
-    if (k < 2) {
-        if (bt == 1) return 3 - k;                 // reflect
-        if (bt == 2) return DIR == 1 ? 2 : 4;      // "absorb" (x: col 2, y: row 4)
-        return nl + k;                             // periodic
-    }
-    if (bt == 1) return 2 * nl + 3 - k;
-    if (bt == 2) return DIR == 1 ? nl + 2 : nl + 1;
-    return k - nl;
-}
-
-template <int DIR>
-__device__ __forceinline__ Cons load_interior(const SweepArgs& a, const LineGeom<DIR>& g, int k) {
-    constexpr int mn = Slots<DIR>::mn, mt = Slots<DIR>::mt;
-    const double* __restrict__ p = a.in + g.at(k);
-    return Cons{__ldg(p), __ldg(p + mn * a.vs), __ldg(p + mt * a.vs), __ldg(p + 3 * a.vs)};
-}
-
-template <int DIR>
-__device__ __forceinline__ Cons load_cell(const SweepArgs& a, const LineGeom<DIR>& g, int k) {
-    constexpr int mn = Slots<DIR>::mn, mt = Slots<DIR>::mt;
-    const long long vs = a.vs;
-    if (k >= 2 && k < a.n - 2) return load_interior<DIR>(a, g, k);
-    // Ghost cell: the fused make_boundary.
-    const int bt = (k < 2) ? a.bnd_lo : a.bnd_hi;
-    const int src = ghost_source<DIR>(bt, k, a.n);
-    double v[4];
-    if (src < 0) {
-        const double* p = a.resid + g.at(k);
-        for (int s = 0; s < 4; s++) v[s] = p[s * vs];
-    } else {
-        const bool interior = src >= 2 && src < a.n - 2;
-        const double* p = (interior ? a.in : a.resid) + g.at(src);
-        const double sn = (bt == 1) ? -1.0 : 1.0;  // reflect flips the normal momentum
-        for (int s = 0; s < 4; s++) v[s] = p[s * vs] * (s == mn ? sn : 1.0);
-        if (a.gout) {
-            double* q = a.gout + g.at(k);
-            for (int s = 0; s < 4; s++) q[s * vs] = v[s];
-        }
-    }
-    return Cons{v[0], v[mn], v[mt], v[3]};
-}
-
-template <int DIR>
-__device__ __forceinline__ void store_cell(const SweepArgs& a, const LineGeom<DIR>& g, int k,
-                                           const Cons& o) {
-    constexpr int mn = Slots<DIR>::mn, mt = Slots<DIR>::mt;
-    double* p = a.out + g.at(k);
-    p[0] = o.d;
-    p[mn * a.vs] = o.mn;
-    p[mt * a.vs] = o.mt;
-    p[3 * a.vs] = o.e;
-}
-
-__device__ __forceinline__ void warp_max_atomic(unsigned long long* dst, double v) {
-    for (int o = 16; o > 0; o >>= 1) v = omax(v, __shfl_xor_sync(0xffffffffu, v, o));
-    if ((threadIdx.x & 31) == 0) atomicMax(dst, (unsigned long long)__double_as_longlong(v));
-}
 
 template <int DIR, bool UNIT>
 __global__ void __launch_bounds__(kSweepThreads)
 sweep_kernel(const SweepArgs a, const Phys P) {
-    const int l = blockIdx.x * blockDim.x + threadIdx.x;
-    bool active = l < a.nlines;
-    double dt = a.dt;
-    if (a.clk) {
-        active = active && a.clk->active;
-        dt = a.clk->dt;
-    }
-    double cx = 0.0, cy = 0.0;  // fused Courant maxima of this thread
-    if (active) {
-        const LineGeom<DIR> g(a, l);
-        const double dtdx = dt / P.dx;
-        const TraceK K = trace_constants(P.scheme, dtdx);
-        const int k0 = 2 + blockIdx.y * a.seg;
-        const int k1 = min(k0 + a.seg, a.n - 2);
-
-        Prim q1, q2;        // primitives of k-1, k-2
-        double c1 = 0.0;    // sound speed of k-1
-        Prim xm2;           // qxm of k-2
-        Cons fprev;         // flux at (k-3 | k-2)
-        q1 = q2 = xm2 = Prim{0.0, 0.0, 0.0, 0.0};
-        fprev = Cons{0.0, 0.0, 0.0, 0.0};
-
-        for (int k = k0 - 2; k <= k1 + 1; k++) {
-            const Cons uk = load_cell<DIR>(a, g, k);
-            Prim qk;
-            double ck;
-            cons_to_prim(P, uk, qk, ck);
-            Prim xm1 = xm2;
-            Cons f = fprev;
-            if (k >= k0) {
-                Prim dq{0.0, 0.0, 0.0, 0.0};
-                if (P.iorder != 1) slope4<UNIT>(P.slope_type, q2, q1, qk, dq);
-                Prim xp1;
-                trace1(K, q1, dq, c1, xm1, xp1);
-                if (k >= k0 + 1) {
-                    f = riemann_flux(P, xm2, xp1);
-                    if (k >= k0 + 2) {
-                        // Cell k-2 is interior: its conservative values are read
-                        // again (an L1/L2 hit) instead of being carried.
-                        const Cons u2 = load_interior<DIR>(a, g, k - 2);
-                        const Cons o = update(u2, fprev, f, dtdx);
-                        store_cell<DIR>(a, g, k - 2, o);
-                        if (a.courant) {
-                            double cn, ct;
-                            courant_speeds(P, o, cn, ct);
-                            if (DIR == 1) {
-                                cx = omax(cx, cn);
-                                cy = omax(cy, ct);
-                            } else {
-                                cx = omax(cx, ct);
-                                cy = omax(cy, cn);
-                            }
-                        }
-                    }
-                }
-            }
-            q2 = q1;
-            q1 = qk;
-            c1 = ck;
-            xm2 = xm1;
-            fprev = f;
-        }
-    }
-    if (a.courant) {
-        warp_max_atomic(&a.courant[0], cx);
-        warp_max_atomic(&a.courant[1], cy);
-    }
+    sweep_body<DIR, ExactStages<UNIT>>(a, P);
 }
 
 cudaError_t launch_sweep(int dir, const SweepArgs& a, const Phys& P, cudaStream_t s) {

@@ -43,6 +43,9 @@ constexpr int kSweepThreads = 64;
 cudaError_t launch_sweep(int dir, const SweepArgs& a, const Phys& P, cudaStream_t s);
 // Resident sweep CTAs per SM (cudaOccupancyMaxActiveBlocksPerMultiprocessor).
 int sweep_blocks_per_sm(int dir, bool unit_slope);
+// The mixed-precision sweep (hb_mixed.cu).
+cudaError_t launch_sweep_mixed(int dir, const SweepArgs& a, const Phys& P, cudaStream_t s);
+int sweep_mixed_blocks_per_sm(int dir);
 cudaError_t launch_courant(const double* u, int nx, int ny, int nxt, long long vs, const Phys& P,
                            unsigned long long* cour, cudaStream_t s);
 cudaError_t launch_boundary(double* u, int idim, int nx, int ny, int nxt, int nyt, long long vs,

@@ -1,0 +1,195 @@
+// hb_march.cuh -- the line-marching skeleton shared by the sweep kernels.
+//
+// One thread owns a segment [k0, k1) of one line (a row for the x sweep, a
+// column for the y sweep) and marches along it with a five-cell window:
+//
+//   iteration k: load cell k (fused make_boundary for ghost cells), its
+//                primitives; slope + trace of cell k-1; Riemann problem + flux
+//                at the interface (k-2 | k-1); update of cell k-2 with the
+//                fluxes on its two faces; store.
+//
+// The arithmetic of each stage comes from a stage set S (hb_stages.cuh: the
+// FP64 restatement of the reference; hb_stages_mixed.cuh: the mixed-precision
+// form).  The state is always FP64 in HBM: 4 doubles read and 4 written per
+// cell and sweep, plus a 4-cell halo per segment.
+#pragma once
+
+#include "hb_kernels.cuh"
+
+namespace hb {
+
+template <int DIR>
+struct LineGeom {
+    // DIR 1: line = row j = l + 2, cells along x.  DIR 2: line = column i = l + 2.
+    long long base;   // offset of cell k = 0 of the line, variable 0
+    long long step;   // offset between consecutive cells of the line
+    __device__ __forceinline__ LineGeom(const SweepArgs& a, int l) {
+        if (DIR == 1) {
+            base = (long long)a.nxt * (l + 2);
+            step = 1;
+        } else {
+            base = l + 2;
+            step = a.nxt;
+        }
+    }
+    __device__ __forceinline__ long long at(int k) const { return base + step * k; }
+};
+
+// Slots of the normal and transverse momentum: IU/IV for x, IV/IU for y
+// (the swap of conservar.c:97-100 and :215-222).
+template <int DIR> struct Slots;
+template <> struct Slots<1> { static constexpr int mn = 1, mt = 2; };
+template <> struct Slots<2> { static constexpr int mn = 2, mt = 1; };
+
+// Ghost source of make_boundary.c:53-198 for position k of a line of n cells
+// (nl = n - 4 interior cells).  Returns -1 when the side has no boundary fill.
+template <int DIR>
+__device__ __forceinline__ int ghost_source(int bt, int k, int n) {
+    const int nl = n - 4;
+    if (bt <= 0) return -1;
+    if (k < 2) {
+        if (bt == 1) return 3 - k;                 // reflect
+        if (bt == 2) return DIR == 1 ? 2 : 4;      // "absorb" (x: col 2, y: row 4)
+        return nl + k;                             // periodic
+    }
+    if (bt == 1) return 2 * nl + 3 - k;
+    if (bt == 2) return DIR == 1 ? nl + 2 : nl + 1;
+    return k - nl;
+}
+
+template <int DIR>
+__device__ __forceinline__ Cons load_interior(const SweepArgs& a, const LineGeom<DIR>& g, int k) {
+    constexpr int mn = Slots<DIR>::mn, mt = Slots<DIR>::mt;
+    const double* __restrict__ p = a.in + g.at(k);
+    return Cons{__ldg(p), __ldg(p + mn * a.vs), __ldg(p + mt * a.vs), __ldg(p + 3 * a.vs)};
+}
+
+template <int DIR>
+__device__ __forceinline__ Cons load_cell(const SweepArgs& a, const LineGeom<DIR>& g, int k) {
+    constexpr int mn = Slots<DIR>::mn, mt = Slots<DIR>::mt;
+    const long long vs = a.vs;
+    if (k >= 2 && k < a.n - 2) return load_interior<DIR>(a, g, k);
+    // Ghost cell: the fused make_boundary.
+    const int bt = (k < 2) ? a.bnd_lo : a.bnd_hi;
+    const int src = ghost_source<DIR>(bt, k, a.n);
+    double v[4];
+    if (src < 0) {
+        const double* p = a.resid + g.at(k);
+        for (int s = 0; s < 4; s++) v[s] = p[s * vs];
+    } else {
+        const bool interior = src >= 2 && src < a.n - 2;
+        const double* p = (interior ? a.in : a.resid) + g.at(src);
+        const double sn = (bt == 1) ? -1.0 : 1.0;  // reflect flips the normal momentum
+        for (int s = 0; s < 4; s++) v[s] = p[s * vs] * (s == mn ? sn : 1.0);
+        if (a.gout) {
+            double* q = a.gout + g.at(k);
+            for (int s = 0; s < 4; s++) q[s * vs] = v[s];
+        }
+    }
+    return Cons{v[0], v[mn], v[mt], v[3]};
+}
+
+template <int DIR>
+__device__ __forceinline__ void store_cell(const SweepArgs& a, const LineGeom<DIR>& g, int k,
+                                           const Cons& o) {
+    constexpr int mn = Slots<DIR>::mn, mt = Slots<DIR>::mt;
+    double* p = a.out + g.at(k);
+    p[0] = o.d;
+    p[mn * a.vs] = o.mn;
+    p[mt * a.vs] = o.mt;
+    p[3 * a.vs] = o.e;
+}
+
+__device__ __forceinline__ void warp_max_atomic(unsigned long long* dst, double v) {
+    for (int o = 16; o > 0; o >>= 1) {
+        const double w = __shfl_xor_sync(0xffffffffu, v, o);
+        v = v > w ? v : w;
+    }
+    if ((threadIdx.x & 31) == 0) atomicMax(dst, (unsigned long long)__double_as_longlong(v));
+}
+
+// The march of one thread over [k0, k1); S::Prim / S::Flux are the stage set's
+// primitive and flux records, S::Real its sound-speed type.
+template <int DIR, class S>
+__device__ __forceinline__ void march(const SweepArgs& a, const typename S::Consts& C,
+                                      const LineGeom<DIR>& g, int k0, int k1, double dtdx,
+                                      double& cx, double& cy) {
+    using Prim = typename S::Prim;
+    using Flux = typename S::Flux;
+    using Real = typename S::Real;
+    const typename S::TraceK K = S::trace_constants(C, dtdx);
+
+    Prim q1 = S::zero_prim(), q2 = S::zero_prim();  // primitives of k-1, k-2
+    Real c1 = Real(0);                              // sound speed of k-1
+    Prim xm2 = S::zero_prim();                      // qxm of k-2
+    Flux fprev = S::zero_flux();                    // flux at (k-3 | k-2)
+
+    for (int k = k0 - 2; k <= k1 + 1; k++) {
+        const Cons uk = load_cell<DIR>(a, g, k);
+        Prim qk;
+        Real ck;
+        S::prim(C, uk, qk, ck);
+        Prim xm1 = xm2;
+        Flux f = fprev;
+        if (k >= k0) {
+            Prim dq = S::zero_prim();
+            if (S::second_order(C)) S::slope4(C, q2, q1, qk, dq);
+            Prim xp1;
+            S::trace(K, q1, dq, c1, xm1, xp1);
+            if (k >= k0 + 1) {
+                f = S::riemann(C, xm2, xp1);
+                if (k >= k0 + 2) {
+                    // Cell k-2 is interior: its conservative values are read
+                    // again (a cache hit) instead of being carried.
+                    const Cons u2 = load_interior<DIR>(a, g, k - 2);
+                    const Cons o = S::update(u2, fprev, f, dtdx);
+                    store_cell<DIR>(a, g, k - 2, o);
+                    if (a.courant) {
+                        double cn, ct;
+                        S::courant(C, o, cn, ct);
+                        if (DIR == 1) {
+                            cx = cx > cn ? cx : cn;
+                            cy = cy > ct ? cy : ct;
+                        } else {
+                            cx = cx > ct ? cx : ct;
+                            cy = cy > cn ? cy : cn;
+                        }
+                    }
+                }
+            }
+        }
+        q2 = q1;
+        q1 = qk;
+        c1 = ck;
+        xm2 = xm1;
+        fprev = f;
+    }
+}
+
+// The sweep kernel body: line and segment from the launch grid, dt from the
+// device clock or the argument, fused Courant reduction.
+template <int DIR, class S>
+__device__ __forceinline__ void sweep_body(const SweepArgs& a, const Phys& P) {
+    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    bool active = l < a.nlines;
+    double dt = a.dt;
+    if (a.clk) {
+        active = active && a.clk->active;
+        dt = a.clk->dt;
+    }
+    double cx = 0.0, cy = 0.0;
+    if (active) {
+        const typename S::Consts C = S::consts(P);
+        const LineGeom<DIR> g(a, l);
+        const double dtdx = dt / P.dx;
+        const int k0 = 2 + blockIdx.y * a.seg;
+        const int k1 = min(k0 + a.seg, a.n - 2);
+        march<DIR, S>(a, C, g, k0, k1, dtdx, cx, cy);
+    }
+    if (a.courant) {
+        warp_max_atomic(&a.courant[0], cx);
+        warp_max_atomic(&a.courant[1], cy);
+    }
+}
+
+}  // namespace hb

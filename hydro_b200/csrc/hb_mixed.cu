@@ -1,0 +1,35 @@
+// hb_mixed.cu -- the mixed-precision sweep kernel (stage set in
+// hb_stages_mixed.cuh, march skeleton in hb_march.cuh).  Built with fast FP32
+// division / square root and FMA contraction (see the Makefile).
+#include "hb_kernels.cuh"
+#include "hb_march.cuh"
+#include "hb_stages_mixed.cuh"
+
+namespace hb {
+
+template <int DIR>
+__global__ void __launch_bounds__(kSweepThreads)
+sweep_mixed_kernel(const SweepArgs a, const Phys P) {
+    sweep_body<DIR, MixedStages>(a, P);
+}
+
+cudaError_t launch_sweep_mixed(int dir, const SweepArgs& a, const Phys& P, cudaStream_t s) {
+    const int nl = a.n - 4;
+    dim3 grid((a.nlines + kSweepThreads - 1) / kSweepThreads, (nl + a.seg - 1) / a.seg);
+    if (dir == 1)
+        sweep_mixed_kernel<1><<<grid, kSweepThreads, 0, s>>>(a, P);
+    else
+        sweep_mixed_kernel<2><<<grid, kSweepThreads, 0, s>>>(a, P);
+    return cudaGetLastError();
+}
+
+int sweep_mixed_blocks_per_sm(int dir) {
+    int n = 0;
+    cudaError_t e = dir == 1 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                                   &n, sweep_mixed_kernel<1>, kSweepThreads, 0)
+                             : cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                                   &n, sweep_mixed_kernel<2>, kSweepThreads, 0);
+    return (e == cudaSuccess && n > 0) ? n : 1;
+}
+
+}  // namespace hb

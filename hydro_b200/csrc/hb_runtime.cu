@@ -81,7 +81,8 @@ struct hb_domain {
     double courant_factor = 0.0;
     int bnd_left = 1, bnd_right = 1, bnd_down = 1, bnd_up = 1;
     int sm_count = 148;
-    int seg[3] = {0, 64, 64};  // output cells per thread segment, per sweep direction
+    int precision = HB_PREC_FP64;
+    int seg[2][3] = {{0, 64, 64}, {0, 64, 64}};  // [precision][direction] segment lengths
     bool cour_valid = false;  // cour holds the maxima of the current state
     int h_nstep = 0;          // host view of the clock's nstep (parity of launches)
     long long launches = 0;
@@ -184,8 +185,14 @@ static int domain_alloc(hb_domain* d) {
     HB_CU(cudaGetDevice(&d->device));
     HB_CU(cudaDeviceGetAttribute(&d->sm_count, cudaDevAttrMultiProcessorCount, d->device));
     for (int dir = 1; dir <= 2; dir++) {
-        const int slots = d->sm_count * hb::sweep_blocks_per_sm(dir, d->P.unit_slope != 0);
-        d->seg[dir] = dir == 1 ? choose_seg(d->ny, d->nx, slots) : choose_seg(d->nx, d->ny, slots);
+        for (int prec = 0; prec < 2; prec++) {
+            const int per_sm = prec == HB_PREC_FP64
+                                   ? hb::sweep_blocks_per_sm(dir, d->P.unit_slope != 0)
+                                   : hb::sweep_mixed_blocks_per_sm(dir);
+            const int slots = d->sm_count * per_sm;
+            d->seg[prec][dir] =
+                dir == 1 ? choose_seg(d->ny, d->nx, slots) : choose_seg(d->nx, d->ny, slots);
+        }
     }
     HB_CU(cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking));
     HB_CU(cudaMalloc(&d->A, d->nelem * sizeof(double)));
@@ -266,7 +273,7 @@ static SweepArgs sweep_args(hb_domain* d, int dir, const double* in, double* out
         a.nlines = d->nx;
         a.n = d->nyt;
     }
-    a.seg = d->seg[dir];
+    a.seg = d->seg[d->precision][dir];
     return a;
 }
 
@@ -288,7 +295,11 @@ static int launch_sweep_timed(hb_domain* d, int dir, const SweepArgs& a) {
         e1 = take_event(d);
         HB_CU(cudaEventRecord(e0, d->stream));
     }
-    HB_CU(hb::launch_sweep(dir, a, d->P, d->stream));
+    if (d->precision == HB_PREC_MIXED) {
+        HB_CU(hb::launch_sweep_mixed(dir, a, d->P, d->stream));
+    } else {
+        HB_CU(hb::launch_sweep(dir, a, d->P, d->stream));
+    }
     d->launches += 1;
     if (d->prof) {
         HB_CU(cudaEventRecord(e1, d->stream));
@@ -322,6 +333,15 @@ extern "C" int hydro_b200_domain_godunov(hb_domain* d, int idim, double dt, int 
     if (!d) return set_error(HB_ERR_ARG, "null domain");
     if (idim != 1 && idim != 2) return set_error(HB_ERR_ARG, "idim=%d: expected 1 or 2", idim);
     return domain_step(d, idim, dt, nullptr, fuse_courant != 0);
+}
+
+extern "C" int hydro_b200_domain_set_precision(hb_domain* d, int precision) {
+    if (!d) return set_error(HB_ERR_ARG, "null domain");
+    if (precision != HB_PREC_FP64 && precision != HB_PREC_MIXED)
+        return set_error(HB_ERR_ARG, "precision=%d: expected HB_PREC_FP64 or HB_PREC_MIXED",
+                         precision);
+    d->precision = precision;
+    return HB_OK;
 }
 
 extern "C" int hydro_b200_domain_profile(hb_domain* d, int enable) {
@@ -508,6 +528,8 @@ static hb_domain* mirror_for(const hydroparam_t* H, hydrovar_t* Hv) {
     }
     hb_domain* d = hydro_b200_domain_create(H);
     if (!d) return nullptr;
+    const char* prec = getenv("HYDRO_B200_PRECISION");
+    if (prec && strcmp(prec, "mixed") == 0) d->precision = HB_PREC_MIXED;
     if (hydro_b200_domain_upload(d, Hv->uold) != HB_OK) {
         hydro_b200_domain_destroy(d);
         return nullptr;

@@ -275,4 +275,43 @@ __device__ __forceinline__ void courant_speeds(const Phys& P, const Cons& u, dou
     ct = c + fabs(q.v);
 }
 
+// The exact FP64 stage set used by the plain sweep (hb_march.cuh).
+template <bool UNIT>
+struct ExactStages {
+    using Consts = Phys;
+    using Prim = hb::Prim;
+    using Flux = Cons;
+    using Real = double;
+    using TraceK = hb::TraceK;
+    static __device__ __forceinline__ Consts consts(const Phys& P) { return P; }
+    static __device__ __forceinline__ Prim zero_prim() { return Prim{0.0, 0.0, 0.0, 0.0}; }
+    static __device__ __forceinline__ Flux zero_flux() { return Flux{0.0, 0.0, 0.0, 0.0}; }
+    static __device__ __forceinline__ TraceK trace_constants(const Phys& P, double dtdx) {
+        return hb::trace_constants(P.scheme, dtdx);
+    }
+    static __device__ __forceinline__ bool second_order(const Phys& P) { return P.iorder != 1; }
+    static __device__ __forceinline__ void prim(const Phys& P, const Cons& u, Prim& q, double& c) {
+        cons_to_prim(P, u, q, c);
+    }
+    static __device__ __forceinline__ void slope4(const Phys& P, const Prim& a, const Prim& b,
+                                                  const Prim& c, Prim& dq) {
+        hb::slope4<UNIT>(P.slope_type, a, b, c, dq);
+    }
+    static __device__ __forceinline__ void trace(const TraceK& K, const Prim& q, const Prim& dq,
+                                                 double c, Prim& xm, Prim& xp) {
+        trace1(K, q, dq, c, xm, xp);
+    }
+    static __device__ __forceinline__ Flux riemann(const Phys& P, const Prim& l, const Prim& r) {
+        return riemann_flux(P, l, r);
+    }
+    static __device__ __forceinline__ Cons update(const Cons& u, const Flux& fl, const Flux& fr,
+                                                  double dtdx) {
+        return hb::update(u, fl, fr, dtdx);
+    }
+    static __device__ __forceinline__ void courant(const Phys& P, const Cons& u, double& cn,
+                                                   double& ct) {
+        courant_speeds(P, u, cn, ct);
+    }
+};
+
 }  // namespace hb

@@ -1,0 +1,270 @@
+// hb_stages_mixed.cuh -- the mixed-precision stage set of the sweep.
+//
+// Same algorithm as the FP64 restatement (hb_stages.cuh, reference citations
+// there), with the precision split:
+//   FP32: constoprim, equation_of_state, slope, trace, the Riemann first guess
+//         and state sampling, cmpflx;
+//   FP64: the Newton iteration on the star pressure (riemann.c:126-156), the
+//         conservative update u + dt/dx (F_l - F_r) with the flux difference
+//         taken in FP64 from the FP32 fluxes, and the Courant speeds that feed
+//         the dt reduction.
+// The state in HBM stays FP64.  This translation unit is built with fast FP32
+// division / square root and FMA contraction; it is not bitwise comparable to
+// the reference and is validated by its L1 / Linf error against the FP64 path.
+#pragma once
+
+#include "hb_kernels.cuh"
+
+namespace hb {
+
+struct PrimF {
+    float r, u, v, p;
+};
+
+struct FluxF {
+    float d, mn, mt, e;
+};
+
+struct MixedConsts {
+    float gamma, gm1, smallr, smallc, smallp, gamma6, entho, slope_type;
+    double gamma6d, smallppd;                 // Newton iteration
+    double gammad, gm1d, smallrd, smallpd;    // Courant speeds
+    int niter, iorder, scheme;
+};
+
+struct TraceKF {
+    float dtdx, zerol, zeror, project;
+};
+
+// Reciprocal and reciprocal square root in FP64 by Newton-Raphson from the
+// FP32 hardware approximation (about 23 correct bits; each step doubles them,
+// two steps reach the FP64 rounding level).  Valid for |x| in the normal
+// FP32 range, which every positive quantity of a valid state is in (the
+// smallest pressure is rho * smallc^2 / gamma >= ~1e-31).
+__device__ __forceinline__ double rcp64(double x) {
+    double y = (double)(1.0f / (float)x);
+    double e = fma(-x, y, 1.0);
+    y = fma(y, e, y);
+    e = fma(-x, y, 1.0);
+    return fma(y, e, y);
+}
+
+__device__ __forceinline__ double rsqrt64(double x) {
+    double y = (double)rsqrtf((float)x);
+    double h = 0.5 * y;
+    double r = fma(-(x * y), h, 0.5);  // 1/2 - x y^2 / 2
+    y = fma(y, r, y);
+    h = 0.5 * y;
+    r = fma(-(x * y), h, 0.5);
+    return fma(y, r, y);
+}
+
+struct MixedStages {
+    using Consts = MixedConsts;
+    using Prim = PrimF;
+    using Flux = FluxF;
+    using Real = float;
+    using TraceK = TraceKF;
+
+    static __device__ __forceinline__ Consts consts(const Phys& P) {
+        Consts C;
+        C.gamma = (float)P.gamma;
+        C.gm1 = (float)P.gm1;
+        C.smallr = (float)P.smallr;
+        C.smallc = (float)P.smallc;
+        C.smallp = (float)P.smallp;
+        C.gamma6 = (float)P.gamma6;
+        C.entho = (float)P.entho;
+        C.slope_type = (float)P.slope_type;
+        C.gamma6d = P.gamma6;
+        C.smallppd = P.smallpp;
+        C.gammad = P.gamma;
+        C.gm1d = P.gm1;
+        C.smallrd = P.smallr;
+        C.smallpd = P.smallp;
+        C.niter = P.niter;
+        C.iorder = P.iorder;
+        C.scheme = P.scheme;
+        return C;
+    }
+    static __device__ __forceinline__ Prim zero_prim() { return Prim{0.f, 0.f, 0.f, 0.f}; }
+    static __device__ __forceinline__ Flux zero_flux() { return Flux{0.f, 0.f, 0.f, 0.f}; }
+    static __device__ __forceinline__ bool second_order(const Consts& C) { return C.iorder != 1; }
+
+    static __device__ __forceinline__ TraceK trace_constants(const Consts& C, double dtdx) {
+        TraceK k;
+        k.dtdx = (float)dtdx;
+        k.zerol = 0.f;
+        k.zeror = 0.f;
+        k.project = 0.f;
+        if (C.scheme == 1) {
+            k.zerol = (float)(-100.0 / dtdx);
+            k.zeror = (float)(100.0 / dtdx);
+            k.project = 1.f;
+        }
+        if (C.scheme == 2) k.project = 1.f;
+        return k;
+    }
+
+    static __device__ __forceinline__ void prim(const Consts& C, const Cons& u, Prim& q, float& c) {
+        const float r = fmaxf((float)u.d, C.smallr);
+        const float ir = 1.0f / r;
+        const float un = (float)u.mn * ir;
+        const float ut = (float)u.mt * ir;
+        const float eken = 0.5f * (un * un + ut * ut);
+        const float e = (float)u.e * ir - eken;
+        const float p = fmaxf(C.gm1 * r * e, r * C.smallp);
+        q = Prim{r, un, ut, p};
+        c = sqrtf(C.gamma * p * ir);
+    }
+
+    static __device__ __forceinline__ float slope1(float st, float qm, float q0, float qp) {
+        const float dlft = st * (q0 - qm);
+        const float drgt = st * (qp - q0);
+        const float dcen = 0.5f * (dlft + drgt) / st;
+        const float lim = (dlft * drgt <= 0.f) ? 0.f : fminf(fabsf(dlft), fabsf(drgt));
+        const float m = fminf(lim, fabsf(dcen));
+        return dcen > 0.f ? m : -m;
+    }
+    static __device__ __forceinline__ void slope4(const Consts& C, const Prim& a, const Prim& b,
+                                                  const Prim& c, Prim& dq) {
+        dq.r = slope1(C.slope_type, a.r, b.r, c.r);
+        dq.u = slope1(C.slope_type, a.u, b.u, c.u);
+        dq.v = slope1(C.slope_type, a.v, b.v, c.v);
+        dq.p = slope1(C.slope_type, a.p, b.p, c.p);
+    }
+
+    static __device__ __forceinline__ void trace(const TraceK& K, const Prim& q, const Prim& dq,
+                                                 float cc, Prim& qxm, Prim& qxp) {
+        const float csq = cc * cc;
+        const float ir = 1.0f / q.r;
+        const float icc = 1.0f / cc;
+        const float rOcc = q.r * icc;
+        const float OrOcc = cc * ir;
+        const float dprcc = dq.p * ir * icc;
+        const float alpham = 0.5f * (dprcc - dq.u) * rOcc;
+        const float alphap = 0.5f * (dprcc + dq.u) * rOcc;
+        const float alpha0r = dq.r - dq.p * icc * icc;
+        const float alpha0v = dq.v;
+        const float upcc = q.u + cc, umcc = q.u - cc;
+        const float upccx = upcc * K.dtdx, umccx = umcc * K.dtdx, ux = q.u * K.dtdx;
+
+        float spm = (umcc >= K.zeror) ? K.project : umccx + 1.f;
+        float spp = (upcc >= K.zeror) ? K.project : upccx + 1.f;
+        float spz = (q.u >= K.zeror) ? K.project : ux + 1.f;
+        float ap = -0.5f * spp * alphap, am = -0.5f * spm * alpham;
+        float azr = -0.5f * spz * alpha0r, azv = -0.5f * spz * alpha0v;
+        qxp = Prim{q.r + (ap + am + azr), q.u + (ap - am) * OrOcc, q.v + azv,
+                   q.p + (ap + am) * csq};
+
+        spm = (umcc <= K.zerol) ? -K.project : umccx - 1.f;
+        spp = (upcc <= K.zerol) ? -K.project : upccx - 1.f;
+        spz = (q.u <= K.zerol) ? -K.project : ux - 1.f;
+        ap = -0.5f * spp * alphap;
+        am = -0.5f * spm * alpham;
+        azr = -0.5f * spz * alpha0r;
+        azv = -0.5f * spz * alpha0v;
+        qxm = Prim{q.r + (ap + am + azr), q.u + (ap - am) * OrOcc, q.v + azv,
+                   q.p + (ap + am) * csq};
+    }
+
+    static __device__ __forceinline__ Flux riemann(const Consts& C, const Prim& ql, const Prim& qr) {
+        // First guess (FP32).
+        const float rl = fmaxf(ql.r, C.smallr), ul = ql.u, pl = fmaxf(ql.p, rl * C.smallp);
+        const float rr = fmaxf(qr.r, C.smallr), ur = qr.u, pr = fmaxf(qr.p, rr * C.smallp);
+        const float cl = C.gamma * pl * rl, cr = C.gamma * pr * rr;
+        const float wl0 = sqrtf(cl), wr0 = sqrtf(cr);
+        const float p0 = fmaxf(((wr0 * pl + wl0 * pr) + wl0 * wr0 * (ul - ur)) / (wl0 + wr0), 0.f);
+
+        // Newton iteration on p* (FP64): W^2 = c (1 + gamma6 (p - p_K) / p_K),
+        // u*_l = u_l - (p - p_l) / W_l, u*_r = u_r + (p - p_r) / W_r, step
+        // dp = (q_l q_r / (q_l + q_r)) (u*_l - u*_r) with q = 2 W^3 / (W^2 + c).
+        const double pld = pl, prd = pr, cld = cl, crd = cr, uld = ul, urd = ur;
+        const double kl = cld * C.gamma6d * rcp64(pld);
+        const double kr = crd * C.gamma6d * rcp64(prd);
+        double pst = p0;
+        for (int iter = 0; iter < C.niter; iter++) {
+            const double wl2 = fma(kl, pst - pld, cld);
+            const double wr2 = fma(kr, pst - prd, crd);
+            const double il = rsqrt64(wl2), ir = rsqrt64(wr2);
+            const double usl = fma(-(pst - pld), il, uld);
+            const double usr = fma(pst - prd, ir, urd);
+            const double iql = 0.5 * (wl2 + cld) * (il * il * il);
+            const double iqr = 0.5 * (wr2 + crd) * (ir * ir * ir);
+            double delp = (usl - usr) * rcp64(iql + iqr);
+            delp = delp > -pst ? delp : -pst;
+            pst += delp;
+            if (!(fabs(delp) > 1e-6 * fabs(pst + C.smallppd))) break;
+        }
+        const float ps = (float)pst;
+
+        // Sampling (FP32).
+        const float wr = sqrtf(cr * (1.f + C.gamma6 * (ps - pr) / pr));
+        const float wl = sqrtf(cl * (1.f + C.gamma6 * (ps - pl) / pl));
+        const float ustar = 0.5f * (ul + (pl - ps) / wl + ur - (pr - ps) / wr);
+        const bool left = ustar > 0.f;
+        const float sgnm = left ? 1.f : -1.f;
+        const float ro = left ? rl : rr, uo = left ? ul : ur, po = left ? pl : pr;
+        const float wo = left ? wl : wr;
+        const float iro = 1.0f / ro;
+        const float co = fmaxf(C.smallc, sqrtf(fabsf(C.gamma * po * iro)));
+        const float rstar = fmaxf(ro / (1.f + ro * (po - ps) / (wo * wo)), C.smallr);
+        const float cstar = fmaxf(C.smallc, sqrtf(fabsf(C.gamma * ps / rstar)));
+        float spout = co - sgnm * uo;
+        float spin = cstar - sgnm * ustar;
+        const float ushock = wo * iro - sgnm * uo;
+        if (ps >= po) {
+            spin = ushock;
+            spout = ushock;
+        }
+        const float scr = fmaxf(spout - spin, C.smallc + fabsf(spout + spin));
+        const float frac = fmaxf(0.f, fminf(1.f, (1.f + (spout + spin) / scr) * 0.5f));
+        float gr, gu, gp;
+        if (spout < 0.f) {
+            gr = ro;
+            gu = uo;
+            gp = po;
+        } else if (spin > 0.f) {
+            gr = rstar;
+            gu = ustar;
+            gp = ps;
+        } else {
+            gr = frac * rstar + (1.f - frac) * ro;
+            gu = frac * ustar + (1.f - frac) * uo;
+            gp = frac * ps + (1.f - frac) * po;
+        }
+        const float gv = left ? ql.v : qr.v;
+        const float mass = gr * gu;
+        const float ekin = 0.5f * gr * (gu * gu + gv * gv);
+        const float etot = gp * C.entho + ekin;
+        return Flux{mass, mass * gu + gp, mass * gv, gu * (etot + gp)};
+    }
+
+    // FP64 update with the flux difference formed in FP64 (the FP32 fluxes
+    // are exact in FP64, so no digits are lost to cancellation).
+    static __device__ __forceinline__ Cons update(const Cons& u, const Flux& fl, const Flux& fr,
+                                                  double dtdx) {
+        return Cons{fma((double)fl.d - (double)fr.d, dtdx, u.d),
+                    fma((double)fl.mn - (double)fr.mn, dtdx, u.mn),
+                    fma((double)fl.mt - (double)fr.mt, dtdx, u.mt),
+                    fma((double)fl.e - (double)fr.e, dtdx, u.e)};
+    }
+
+    // Courant speeds of the updated cell in FP64 (ComputeQEforRow +
+    // equation_of_state + courantOnXY).
+    static __device__ __forceinline__ void courant(const Consts& C, const Cons& u, double& cn,
+                                                   double& ct) {
+        const double r = u.d > C.smallrd ? u.d : C.smallrd;
+        const double ir = rcp64(r);
+        const double un = u.mn * ir, ut = u.mt * ir;
+        const double e = u.e * ir - 0.5 * (un * un + ut * ut);
+        double p = C.gm1d * r * e;
+        p = p > r * C.smallpd ? p : r * C.smallpd;
+        const double c2 = C.gammad * p * ir;
+        const double c = c2 * rsqrt64(c2);
+        cn = c + fabs(un);
+        ct = c + fabs(ut);
+    }
+};
+
+}  // namespace hb

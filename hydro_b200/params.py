@@ -170,3 +170,37 @@ def init_state(H: HydroParam, testcase: int | None = None, out: np.ndarray | Non
     else:
         raise ValueError("Test case not implemented")
     return u
+
+
+# ---------------------------------------------------------------- seeded inputs
+_SM_GAMMA = np.uint64(0x9E3779B97F4A7C15)
+_SM_M1 = np.uint64(0xBF58476D1CE4E5B9)
+_SM_M2 = np.uint64(0x94D049BB133111EB)
+
+
+def splitmix64(x: np.ndarray) -> np.ndarray:
+    """SplitMix64 finaliser (Steele, Lea & Flood, OOPSLA 2014) on uint64 counters."""
+    with np.errstate(over="ignore"):
+        z = x.astype(np.uint64) + _SM_GAMMA
+        z = (z ^ (z >> np.uint64(30))) * _SM_M1
+        z = (z ^ (z >> np.uint64(27))) * _SM_M2
+        return z ^ (z >> np.uint64(31))
+
+
+def uniform_pm1(seed: int, counters: np.ndarray) -> np.ndarray:
+    """U(-1, 1) doubles from SplitMix64(seed XOR counter), 53-bit mantissas."""
+    z = splitmix64(np.uint64(seed) ^ counters.astype(np.uint64))
+    u = (z >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+    return 2.0 * u - 1.0
+
+
+def init_noisy_blast(H: HydroParam, seed: int, amplitude: float = 0.01, testcase: int = 1):
+    """The test-case state with the interior density scaled by
+    1 + amplitude * U(-1, 1), U drawn per interior cell (counter = j*nx + i,
+    interior coordinates) -- the mixed-precision workload's input."""
+    u = init_state(H, testcase)
+    j, i = np.meshgrid(np.arange(H.ny, dtype=np.uint64), np.arange(H.nx, dtype=np.uint64),
+                       indexing="ij")
+    noise = uniform_pm1(seed, j * np.uint64(H.nx) + i)
+    u[0, 2:-2, 2:-2] *= 1.0 + amplitude * noise
+    return u

@@ -120,13 +120,15 @@ class HydroRun:
 class Domain:
     """Device-resident state (hb_domain)."""
 
-    def __init__(self, H: HydroParam):
+    def __init__(self, H: HydroParam, precision: str = "fp64"):
         self.lib = load()
         self.H = H
         self.h = self.lib.hydro_b200_domain_create(C.byref(H))
         if not self.h:
             check()
             raise _lib.HydroB200Error("domain creation failed")
+        self.precision = precision
+        check(self.lib.hydro_b200_domain_set_precision(self.h, _lib.PRECISIONS[precision]))
         self.shape = state_shape(H)
         self.nbytes = int(np.prod(self.shape)) * 8
 

@@ -184,6 +184,15 @@ int hydro_b200_domain_set_clock(hb_domain *d, double t, int nstep, double dt);
 int hydro_b200_domain_launch_steps(hb_domain *d, int nsteps, int nstepmax, double tend);
 int hydro_b200_domain_get_clock(hb_domain *d, double *t, int *nstep, double *dt); /* synchronous */
 int hydro_b200_domain_get_dts(hb_domain *d, double *dts, int n); /* dt of the steps since set_clock */
+/* Arithmetic of the sweeps.  HB_PREC_FP64 (default): the reference's FP64
+ * operations, bit for bit.  HB_PREC_MIXED: FP32 constoprim / EOS / slope /
+ * trace / Riemann sampling / flux, FP64 Newton iteration on p*, FP64 update
+ * and Courant speeds; the state stays FP64.  Mirrors created through the
+ * reference entry points use HB_PREC_MIXED when HYDRO_B200_PRECISION=mixed. */
+#define HB_PREC_FP64 0
+#define HB_PREC_MIXED 1
+int hydro_b200_domain_set_precision(hb_domain *d, int precision);
+
 /* Event timing of every sweep launch: enable, then read the accumulated
  * milliseconds and launch counts of x (index 0) and y (index 1) sweeps. */
 int hydro_b200_domain_profile(hb_domain *d, int enable);
