@@ -128,6 +128,7 @@ SIGNATURES = [
     ("hydro_b200_domain_profile", C.c_int, [_D, C.c_int]),
     ("hydro_b200_domain_profile_read", C.c_int, [_D, _DP, C.POINTER(C.c_longlong), C.c_int]),
     ("hydro_b200_set_device", C.c_int, [C.c_int]),
+    ("hydro_b200_godunov_noalloc", C.c_int, [_P, C.c_void_p, C.c_int, C.c_double, C.c_void_p]),
     ("hydro_b200_build_info", C.c_char_p, []),
 ]
 

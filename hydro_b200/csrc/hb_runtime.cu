@@ -57,6 +57,9 @@ static int set_error(int code, const char* fmt, ...) {
                              __FILE__, __LINE__);                                        \
     } while (0)
 
+// Records an error from another translation unit of the library.
+int hb_record_error(int code, const char* msg) { return set_error(code, "%s", msg); }
+
 extern "C" int hydro_b200_last_error(void) { return g_err; }
 extern "C" const char* hydro_b200_last_error_message(void) { return g_msg; }
 extern "C" void hydro_b200_clear_error(void) {

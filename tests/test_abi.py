@@ -20,6 +20,7 @@ GOLDEN = os.path.join(ROOT, "tests", "golden", "abi_layout.json")
 def declared_functions():
     src = open(HEADER).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    src = re.sub(r"^\s*#.*$", "", src, flags=re.M)
     names = re.findall(r"\b([A-Za-z_][A-Za-z0-9_]*)\s*\([^;{]*\)\s*;", src)
     return sorted(set(n for n in names if n not in ("if", "while", "sizeof")))
 
