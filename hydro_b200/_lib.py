@@ -20,6 +20,8 @@ MAX_BOX = 8
 HB_OK, HB_ERR_ARG, HB_ERR_CUDA, HB_ERR_NODEV, HB_ERR_NOMEM, HB_ERR_STATE, HB_ERR_TIMEOUT = range(7)
 HB_PREC_FP64, HB_PREC_MIXED = 0, 1
 PRECISIONS = {"fp64": HB_PREC_FP64, "mixed": HB_PREC_MIXED}
+HB_XSWEEP_MARCH, HB_XSWEEP_CELL = 0, 1
+XSWEEPS = {"march": HB_XSWEEP_MARCH, "cell": HB_XSWEEP_CELL}
 
 
 class HydroParam(C.Structure):
@@ -125,6 +127,7 @@ SIGNATURES = [
     ("hydro_b200_domain_get_dts", C.c_int, [_D, _DP, C.c_int]),
     ("hydro_b200_domain_launch_count", C.c_longlong, [_D]),
     ("hydro_b200_domain_set_precision", C.c_int, [_D, C.c_int]),
+    ("hydro_b200_domain_set_xsweep", C.c_int, [_D, C.c_int, C.c_int]),
     ("hydro_b200_domain_profile", C.c_int, [_D, C.c_int]),
     ("hydro_b200_domain_profile_read", C.c_int, [_D, _DP, C.POINTER(C.c_longlong), C.c_int]),
     ("hydro_b200_set_device", C.c_int, [C.c_int]),

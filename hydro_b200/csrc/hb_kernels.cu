@@ -33,6 +33,24 @@ sweep_kernel(const SweepArgs a, const Phys P) {
     sweep_body<DIR, ExactStages<UNIT>>(a, P);
 }
 
+template <bool UNIT>
+__global__ void __launch_bounds__(kCellThreads)
+xcell_kernel(const SweepArgs a, const Phys P) {
+    xcell_body<ExactStages<UNIT>>(a, P);
+}
+
+static dim3 xcell_grid(const SweepArgs& a) {
+    const int nwin = (a.n - 4 + kCellWarpOut - 1) / kCellWarpOut;
+    const int wpc = kCellThreads / 32;
+    return dim3(a.nlines, (nwin + wpc - 1) / wpc);
+}
+
+cudaError_t launch_xcell(const SweepArgs& a, const Phys& P, cudaStream_t s) {
+    if (P.unit_slope) xcell_kernel<true><<<xcell_grid(a), kCellThreads, 0, s>>>(a, P);
+    else xcell_kernel<false><<<xcell_grid(a), kCellThreads, 0, s>>>(a, P);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_sweep(int dir, const SweepArgs& a, const Phys& P, cudaStream_t s) {
     const int nl = a.n - 4;
     dim3 grid((a.nlines + kSweepThreads - 1) / kSweepThreads, (nl + a.seg - 1) / a.seg);

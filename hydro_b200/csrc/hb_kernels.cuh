@@ -43,6 +43,10 @@ constexpr int kSweepThreads = 64;
 cudaError_t launch_sweep(int dir, const SweepArgs& a, const Phys& P, cudaStream_t s);
 // Resident sweep CTAs per SM (cudaOccupancyMaxActiveBlocksPerMultiprocessor).
 int sweep_blocks_per_sm(int dir, bool unit_slope);
+// The x sweep with one cell per lane (hb_march.cuh xcell_body): FP64 and mixed.
+constexpr int kCellThreads = 64;
+cudaError_t launch_xcell(const SweepArgs& a, const Phys& P, cudaStream_t s);
+cudaError_t launch_xcell_mixed(const SweepArgs& a, const Phys& P, cudaStream_t s);
 // The mixed-precision sweep (hb_mixed.cu).
 cudaError_t launch_sweep_mixed(int dir, const SweepArgs& a, const Phys& P, cudaStream_t s);
 int sweep_mixed_blocks_per_sm(int dir);

@@ -108,6 +108,45 @@ __device__ __forceinline__ void warp_max_atomic(unsigned long long* dst, double 
     if ((threadIdx.x & 31) == 0) atomicMax(dst, (unsigned long long)__double_as_longlong(v));
 }
 
+// Row staging of the x sweep.  A thread walking its own row would fetch each
+// 32-byte sector four times (once per cell) from a thrashed L1; instead it
+// fetches the four cells of a sector at once (two 16-byte loads per variable
+// when the row is 16-byte aligned) into its own column of a shared-memory ring
+// of 8 cells, and reads cells (including cell k-2 for the update) back from
+// there.  Each thread touches only its own column, so no barrier is needed.
+struct RowRing {
+    double (*t)[8][kSweepThreads];  // [variable slot][ring position][thread]
+    int tid;
+    __device__ __forceinline__ double& at(int v, int k) { return t[v][k & 7][tid]; }
+    __device__ __forceinline__ Cons cell(int k) {
+        return Cons{at(0, k), at(Slots<1>::mn, k), at(Slots<1>::mt, k), at(3, k)};
+    }
+    // Cells [k, k+4) that are interior and <= kmax.
+    __device__ __forceinline__ void fill(const SweepArgs& a, const LineGeom<1>& g, int k,
+                                         int kmax, bool vec_ok) {
+        const int lo = k > 2 ? k : 2;
+        const int hi = min(min(k + 3, kmax), a.n - 3);
+        if (vec_ok && lo == k && hi == k + 3) {
+            const double* p = a.in + g.at(k);
+#pragma unroll
+            for (int v = 0; v < 4; v++) {
+                const double2 x = __ldg(reinterpret_cast<const double2*>(p + v * a.vs));
+                const double2 y = __ldg(reinterpret_cast<const double2*>(p + v * a.vs) + 1);
+                at(v, k) = x.x;
+                at(v, k + 1) = x.y;
+                at(v, k + 2) = y.x;
+                at(v, k + 3) = y.y;
+            }
+        } else {
+            for (int kk = lo; kk <= hi; kk++) {
+                const double* p = a.in + g.at(kk);
+#pragma unroll
+                for (int v = 0; v < 4; v++) at(v, kk) = __ldg(p + v * a.vs);
+            }
+        }
+    }
+};
+
 // The march of one thread over [k0, k1); S::Prim / S::Flux are the stage set's
 // primitive and flux records, S::Real its sound-speed type.
 template <int DIR, class S>
@@ -119,13 +158,29 @@ __device__ __forceinline__ void march(const SweepArgs& a, const typename S::Cons
     using Real = typename S::Real;
     const typename S::TraceK K = S::trace_constants(C, dtdx);
 
+    __shared__ double ring_mem[DIR == 1 ? 4 : 1][8][kSweepThreads];
+    RowRing ring{ring_mem, (int)threadIdx.x};
+    // 16-byte loads need every address in + base + k + v*vs (in doubles) of a
+    // chunk to be even from a 16-byte aligned pointer: aligned `in`, even
+    // variable stride, even row start and an even first cell (chunks advance
+    // by 4 cells).
+    const bool vec_ok = DIR == 1 && ((reinterpret_cast<uintptr_t>(a.in) & 15) == 0) &&
+                        ((a.vs & 1) == 0) && ((g.base & 1) == 0) && (((k0 - 2) & 1) == 0);
+
     Prim q1 = S::zero_prim(), q2 = S::zero_prim();  // primitives of k-1, k-2
     Real c1 = Real(0);                              // sound speed of k-1
     Prim xm2 = S::zero_prim();                      // qxm of k-2
     Flux fprev = S::zero_flux();                    // flux at (k-3 | k-2)
 
     for (int k = k0 - 2; k <= k1 + 1; k++) {
-        const Cons uk = load_cell<DIR>(a, g, k);
+        Cons uk;
+        if (DIR == 1) {
+            if (((k - (k0 - 2)) & 3) == 0) ring.fill(a, reinterpret_cast<const LineGeom<1>&>(g), k,
+                                                     k1 + 1, vec_ok);
+            uk = (k >= 2 && k < a.n - 2) ? ring.cell(k) : load_cell<DIR>(a, g, k);
+        } else {
+            uk = load_cell<DIR>(a, g, k);
+        }
         Prim qk;
         Real ck;
         S::prim(C, uk, qk, ck);
@@ -140,8 +195,8 @@ __device__ __forceinline__ void march(const SweepArgs& a, const typename S::Cons
                 f = S::riemann(C, xm2, xp1);
                 if (k >= k0 + 2) {
                     // Cell k-2 is interior: its conservative values are read
-                    // again (a cache hit) instead of being carried.
-                    const Cons u2 = load_interior<DIR>(a, g, k - 2);
+                    // again (the row ring, or a cache hit) instead of being carried.
+                    const Cons u2 = DIR == 1 ? ring.cell(k - 2) : load_interior<DIR>(a, g, k - 2);
                     const Cons o = S::update(u2, fprev, f, dtdx);
                     store_cell<DIR>(a, g, k - 2, o);
                     if (a.courant) {
@@ -185,6 +240,88 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, const Phys& P) {
         const int k0 = 2 + blockIdx.y * a.seg;
         const int k1 = min(k0 + a.seg, a.n - 2);
         march<DIR, S>(a, C, g, k0, k1, dtdx, cx, cy);
+    }
+    if (a.courant) {
+        warp_max_atomic(&a.courant[0], cx);
+        warp_max_atomic(&a.courant[1], cy);
+    }
+}
+
+
+// ---------------------------------------------------------------------------
+// The x sweep with one cell per lane.  A warp takes 32 consecutive cells
+// [c - 2, c + 30) of one row, so every load and store instruction covers
+// whole 128-byte lines of the row; neighbours are exchanged with warp
+// shuffles instead of a marching window.  Lanes 2..29 produce the updates of
+// cells [c, c + 28): the halo costs 4 of 32 lanes of arithmetic, against
+// whole-line DRAM traffic (a row-marching thread consumes a line over many
+// iterations and loses it from L2 in between).
+template <class T>
+__device__ __forceinline__ T shfl_up1(T v) { return __shfl_up_sync(0xffffffffu, v, 1); }
+template <class T>
+__device__ __forceinline__ T shfl_down1(T v) { return __shfl_down_sync(0xffffffffu, v, 1); }
+
+template <class P>
+__device__ __forceinline__ P prim_up(const P& q) {
+    return P{shfl_up1(q.r), shfl_up1(q.u), shfl_up1(q.v), shfl_up1(q.p)};
+}
+template <class P>
+__device__ __forceinline__ P prim_down(const P& q) {
+    return P{shfl_down1(q.r), shfl_down1(q.u), shfl_down1(q.v), shfl_down1(q.p)};
+}
+template <class F>
+__device__ __forceinline__ F flux_up(const F& f) {
+    return F{shfl_up1(f.d), shfl_up1(f.mn), shfl_up1(f.mt), shfl_up1(f.e)};
+}
+
+constexpr int kCellWarpOut = 28;  // outputs per warp of the cell-per-lane x sweep
+
+// Grid: x = rows, y = ceil(windows / warps per CTA); window = 28 output cells.
+template <class S>
+__device__ __forceinline__ void xcell_body(const SweepArgs& a, const Phys& P) {
+    using Prim = typename S::Prim;
+    using Flux = typename S::Flux;
+    using Real = typename S::Real;
+    const int lane = threadIdx.x & 31;
+    const int warp = blockIdx.y * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int row = blockIdx.x;                       // interior row index l
+    const int c = 2 + warp * kCellWarpOut;            // first output cell of the warp
+    const int k = c - 2 + lane;                       // this lane's cell
+    bool active = row < a.nlines && c < a.n - 2;      // warp-uniform
+    double dt = a.dt;
+    if (a.clk) {
+        active = active && a.clk->active;
+        dt = a.clk->dt;
+    }
+    double cx = 0.0, cy = 0.0;
+    if (active) {
+        const typename S::Consts C = S::consts(P);
+        const LineGeom<1> g(a, row);
+        const double dtdx = dt / P.dx;
+        const typename S::TraceK K = S::trace_constants(C, dtdx);
+        const bool inside = k < a.n;                  // lanes past the row end idle
+        const Cons u = inside ? load_cell<1>(a, g, k) : Cons{1.0, 0.0, 0.0, 1.0};
+        Prim q;
+        Real cs;
+        S::prim(C, u, q, cs);
+        const Prim qm = prim_up(q), qp = prim_down(q);
+        Prim dq = S::zero_prim();
+        if (S::second_order(C)) S::slope4(C, qm, q, qp, dq);
+        Prim xm, xp;
+        S::trace(K, q, dq, cs, xm, xp);
+        const Prim xp_next = prim_down(xp);           // qxp of cell k + 1
+        const Flux f = S::riemann(C, xm, xp_next);    // interface (k | k + 1)
+        const Flux f_prev = flux_up(f);               // interface (k - 1 | k)
+        if (lane >= 2 && lane < 2 + kCellWarpOut && k < a.n - 2) {
+            const Cons o = S::update(u, f_prev, f, dtdx);
+            store_cell<1>(a, g, k, o);
+            if (a.courant) {
+                double cn, ct;
+                S::courant(C, o, cn, ct);
+                cx = cn;
+                cy = ct;
+            }
+        }
     }
     if (a.courant) {
         warp_max_atomic(&a.courant[0], cx);

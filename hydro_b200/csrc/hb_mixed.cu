@@ -13,6 +13,19 @@ sweep_mixed_kernel(const SweepArgs a, const Phys P) {
     sweep_body<DIR, MixedStages>(a, P);
 }
 
+__global__ void __launch_bounds__(kCellThreads)
+xcell_mixed_kernel(const SweepArgs a, const Phys P) {
+    xcell_body<MixedStages>(a, P);
+}
+
+cudaError_t launch_xcell_mixed(const SweepArgs& a, const Phys& P, cudaStream_t s) {
+    const int nwin = (a.n - 4 + kCellWarpOut - 1) / kCellWarpOut;
+    const int wpc = kCellThreads / 32;
+    dim3 grid(a.nlines, (nwin + wpc - 1) / wpc);
+    xcell_mixed_kernel<<<grid, kCellThreads, 0, s>>>(a, P);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_sweep_mixed(int dir, const SweepArgs& a, const Phys& P, cudaStream_t s) {
     const int nl = a.n - 4;
     dim3 grid((a.nlines + kSweepThreads - 1) / kSweepThreads, (nl + a.seg - 1) / a.seg);

@@ -85,6 +85,7 @@ struct hb_domain {
     int bnd_left = 1, bnd_right = 1, bnd_down = 1, bnd_up = 1;
     int sm_count = 148;
     int precision = HB_PREC_FP64;
+    int xsweep[2] = {HB_XSWEEP_CELL, HB_XSWEEP_CELL};  // x-sweep kernel per precision
     int seg[2][3] = {{0, 64, 64}, {0, 64, 64}};  // [precision][direction] segment lengths
     bool cour_valid = false;  // cour holds the maxima of the current state
     int h_nstep = 0;          // host view of the clock's nstep (parity of launches)
@@ -166,7 +167,9 @@ static int choose_seg(int nlines, int nl, int slots) {
     for (int w = 1; w <= 64; w++) {
         const int nseg_want = (int)((long long)w * slots / groups);
         if (nseg_want < 1) continue;
-        const int seg = (nl + nseg_want - 1) / nseg_want;
+        // Even lengths keep every thread's first cell 16-byte aligned for the
+        // x sweep's vector loads.
+        const int seg = (((nl + nseg_want - 1) / nseg_want) + 1) & ~1;
         if (seg < 24) break;
         const int nseg = (nl + seg - 1) / seg;
         const long long ctas = (long long)groups * nseg;
@@ -298,10 +301,13 @@ static int launch_sweep_timed(hb_domain* d, int dir, const SweepArgs& a) {
         e1 = take_event(d);
         HB_CU(cudaEventRecord(e0, d->stream));
     }
+    const bool cell = dir == 1 && d->xsweep[d->precision] == HB_XSWEEP_CELL;
     if (d->precision == HB_PREC_MIXED) {
-        HB_CU(hb::launch_sweep_mixed(dir, a, d->P, d->stream));
+        HB_CU(cell ? hb::launch_xcell_mixed(a, d->P, d->stream)
+                   : hb::launch_sweep_mixed(dir, a, d->P, d->stream));
     } else {
-        HB_CU(hb::launch_sweep(dir, a, d->P, d->stream));
+        HB_CU(cell ? hb::launch_xcell(a, d->P, d->stream)
+                   : hb::launch_sweep(dir, a, d->P, d->stream));
     }
     d->launches += 1;
     if (d->prof) {
@@ -344,6 +350,15 @@ extern "C" int hydro_b200_domain_set_precision(hb_domain* d, int precision) {
         return set_error(HB_ERR_ARG, "precision=%d: expected HB_PREC_FP64 or HB_PREC_MIXED",
                          precision);
     d->precision = precision;
+    return HB_OK;
+}
+
+extern "C" int hydro_b200_domain_set_xsweep(hb_domain* d, int precision, int mode) {
+    if (!d) return set_error(HB_ERR_ARG, "null domain");
+    if ((precision != HB_PREC_FP64 && precision != HB_PREC_MIXED) ||
+        (mode != HB_XSWEEP_MARCH && mode != HB_XSWEEP_CELL))
+        return set_error(HB_ERR_ARG, "precision=%d mode=%d: invalid", precision, mode);
+    d->xsweep[precision] = mode;
     return HB_OK;
 }
 
@@ -533,6 +548,9 @@ static hb_domain* mirror_for(const hydroparam_t* H, hydrovar_t* Hv) {
     if (!d) return nullptr;
     const char* prec = getenv("HYDRO_B200_PRECISION");
     if (prec && strcmp(prec, "mixed") == 0) d->precision = HB_PREC_MIXED;
+    const char* xs = getenv("HYDRO_B200_XSWEEP");
+    if (xs && strcmp(xs, "cell") == 0) d->xsweep[0] = d->xsweep[1] = HB_XSWEEP_CELL;
+    if (xs && strcmp(xs, "march") == 0) d->xsweep[0] = d->xsweep[1] = HB_XSWEEP_MARCH;
     if (hydro_b200_domain_upload(d, Hv->uold) != HB_OK) {
         hydro_b200_domain_destroy(d);
         return nullptr;

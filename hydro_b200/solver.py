@@ -120,7 +120,7 @@ class HydroRun:
 class Domain:
     """Device-resident state (hb_domain)."""
 
-    def __init__(self, H: HydroParam, precision: str = "fp64"):
+    def __init__(self, H: HydroParam, precision: str = "fp64", xsweep: str | None = None):
         self.lib = load()
         self.H = H
         self.h = self.lib.hydro_b200_domain_create(C.byref(H))
@@ -129,6 +129,9 @@ class Domain:
             raise _lib.HydroB200Error("domain creation failed")
         self.precision = precision
         check(self.lib.hydro_b200_domain_set_precision(self.h, _lib.PRECISIONS[precision]))
+        if xsweep is not None:
+            check(self.lib.hydro_b200_domain_set_xsweep(self.h, _lib.PRECISIONS[precision],
+                                                        _lib.XSWEEPS[xsweep]))
         self.shape = state_shape(H)
         self.nbytes = int(np.prod(self.shape)) * 8
 

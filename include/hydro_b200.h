@@ -193,6 +193,17 @@ int hydro_b200_domain_get_dts(hb_domain *d, double *dts, int n); /* dt of the st
 #define HB_PREC_MIXED 1
 int hydro_b200_domain_set_precision(hb_domain *d, int precision);
 
+/* Kernel of the x sweep.  HB_XSWEEP_MARCH: each thread marches along a row
+ * segment (as the y sweep does along columns).  HB_XSWEEP_CELL: a warp takes
+ * 32 consecutive cells of a row, one per lane, and exchanges neighbours by
+ * shuffles (whole-line memory accesses, 28 of 32 lanes productive).  Both give
+ * identical results; CELL is the default (faster at 4096^2 for both
+ * precisions: the x sweep's loads then use whole lines).  Mirrors
+ * created through the reference entry points use HYDRO_B200_XSWEEP=cell|march. */
+#define HB_XSWEEP_MARCH 0
+#define HB_XSWEEP_CELL 1
+int hydro_b200_domain_set_xsweep(hb_domain *d, int precision, int mode);
+
 /* Event timing of every sweep launch: enable, then read the accumulated
  * milliseconds and launch counts of x (index 0) and y (index 1) sweeps. */
 int hydro_b200_domain_profile(hb_domain *d, int enable);

@@ -77,7 +77,8 @@ def test_reference_golden_runs(product_lib, name):
     (64, 64, 0, 30, (1, 1, 1, 1), {"niter_riemann": 0}),
 ])
 def test_device_loop_matches_oracle(product_lib, oracle, nx, ny, tc, nsteps, bnd, extra):
-    """hydro_b200_run (dt and t on the device) against the oracle."""
+    """hydro_b200_run (dt and t on the device) against the oracle (x sweep:
+    the default cell-per-lane kernel)."""
     H = make_params(nx, ny, boundary=bnd, testcase=tc, **extra)
     want, wdts, wt = run_oracle(oracle, H, tc, nsteps)
     run = HydroRun(H)
@@ -87,6 +88,28 @@ def test_device_loop_matches_oracle(product_lib, oracle, nx, ny, tc, nsteps, bnd
     assert len(dts) == nsteps and bitwise_equal(dts, wdts)
     assert run.t == wt
     assert bitwise_equal(u, want), describe_mismatch(u, want)
+
+
+@pytest.mark.parametrize("nx,ny,tc,nsteps,bnd,extra", [
+    (37, 41, 0, 40, (1, 1, 1, 1), {}),
+    (130, 67, 1, 60, (2, 3, 1, 2), {}),
+    (29, 35, 1, 30, (2, 2, 2, 2), {}),
+    (200, 3, 2, 20, (1, 1, 1, 1), {}),
+    (3, 150, 0, 20, (3, 3, 3, 3), {}),
+    (80, 50, 0, 30, (0, 1, 0, 1), {"iorder": 1, "scheme": 2}),
+    (300, 64, 0, 30, (1, 1, 1, 1), {"slope_type": 0.5}),
+])
+def test_marching_x_sweep_matches_oracle(product_lib, oracle, nx, ny, tc, nsteps, bnd, extra):
+    """The same, with the row-marching x-sweep kernel (shared-memory row ring)."""
+    H = make_params(nx, ny, boundary=bnd, testcase=tc, **extra)
+    want, wdts, wt = run_oracle(oracle, H, tc, nsteps)
+    d = Domain(H, xsweep="march")
+    d.upload(init_state(H, tc))
+    d.set_clock()
+    d.launch_steps(nsteps)
+    got = d.download()
+    d.close()
+    assert bitwise_equal(got, want), describe_mismatch(got, want)
 
 
 def test_device_loop_and_reference_entry_points_agree(product_lib):
