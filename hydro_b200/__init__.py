@@ -10,9 +10,11 @@ from ._lib import (HydroB200Error, HydroParam, HydroVar, HydroVarWork, HydroWork
 from .params import (HSCHEME_COLLELA, HSCHEME_MUSCL, HSCHEME_PLMDE, default_params, finalize,
                      init_state, make_params, read_nml, state_shape)
 from .solver import Domain, HydroRun
+from .batch import Batch, make_blast_mix
 
 __all__ = [
     "HydroB200Error", "HydroParam", "HydroVar", "HydroVarWork", "HydroWork", "LIB_PATH", "load",
     "HSCHEME_COLLELA", "HSCHEME_MUSCL", "HSCHEME_PLMDE", "default_params", "finalize",
     "init_state", "make_params", "read_nml", "state_shape", "Domain", "HydroRun",
+    "Batch", "make_blast_mix",
 ]

@@ -130,6 +130,25 @@ SIGNATURES = [
     ("hydro_b200_domain_set_xsweep", C.c_int, [_D, C.c_int, C.c_int]),
     ("hydro_b200_domain_profile", C.c_int, [_D, C.c_int]),
     ("hydro_b200_domain_profile_read", C.c_int, [_D, _DP, C.POINTER(C.c_longlong), C.c_int]),
+    ("hydro_b200_batch_create", _D, [_P, C.c_int, C.c_size_t, C.c_int]),
+    ("hydro_b200_batch_destroy", None, [_D]),
+    ("hydro_b200_batch_bytes_needed", C.c_longlong, [_P]),
+    ("hydro_b200_batch_arena_free", C.c_longlong, [_D]),
+    ("hydro_b200_batch_add", C.c_int, [_D, _P, C.c_void_p, C.c_double, C.c_int]),
+    ("hydro_b200_batch_remove", C.c_int, [_D, C.c_int]),
+    ("hydro_b200_batch_steps", C.c_int, [_D, C.c_int]),
+    ("hydro_b200_batch_synchronize", C.c_int, [_D]),
+    ("hydro_b200_batch_status", C.c_int, [_D, C.c_int, _DP, C.POINTER(C.c_int), _DP,
+                                          C.POINTER(C.c_int), C.POINTER(C.c_longlong)]),
+    ("hydro_b200_batch_poll", C.c_int, [_D, C.POINTER(C.c_int), C.c_int]),
+    ("hydro_b200_batch_download", C.c_int, [_D, C.c_int, C.c_void_p]),
+    ("hydro_b200_batch_global_step", C.c_longlong, [_D]),
+    ("hydro_b200_batch_launch_count", C.c_longlong, [_D]),
+    ("hydro_b200_batch_stream", C.c_void_p, [_D]),
+    ("hydro_b200_batch_set_tuning", C.c_int, [_D, C.c_int, C.c_int, C.c_int]),
+    ("hydro_b200_batch_get_tuning", C.c_int, [_D, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                              C.POINTER(C.c_int)]),
+    ("hydro_b200_batch_autotune", C.c_int, [_D, C.c_int]),
     ("hydro_b200_set_device", C.c_int, [C.c_int]),
     ("hydro_b200_godunov_noalloc", C.c_int, [_P, C.c_void_p, C.c_int, C.c_double, C.c_void_p]),
     ("hydro_b200_build_info", C.c_char_p, []),

@@ -1,0 +1,69 @@
+// hb_batch.cuh -- many independent HydroC runs advanced together.
+//
+// A batch holds up to `capacity` instances ("slots"), each a grid of its own
+// size with its own state, scratch buffer, clock (t, dt, nstep) and Courant
+// accumulators, all resident in one device arena.  One global step advances
+// every active instance by one time step of its own (main.c:344-408 per
+// instance): a clock kernel (dt on even steps, stop test), two persistent
+// sweep launches that pull work items of all instances from a queue, and a
+// clock kernel (t += dt, nstep++).  Work items are CTA-sized: an x item is
+// one row's run of cell windows (cell-per-lane x sweep), a y item is a group
+// of 64 columns over one row segment (marching y sweep).  Instances need not
+// share the sweep order: each instance's first sweep is x on its even steps
+// and y on its odd ones, so the host builds two item lists from the
+// instances' step parities and the launches alternate them.
+#pragma once
+
+#include "hb_kernels.cuh"
+
+namespace hb {
+
+struct BatchInst {
+    double* A;          // state, reference layout
+    double* B;          // scratch of the same size (first sweep's output)
+    int nx, ny, nxt, nyt;
+    long long vs;
+    int bnd_left, bnd_right, bnd_down, bnd_up;
+    double dx;
+    double t, dt, tend;
+    int nstep, nstepmax;
+    int active;         // 1 while t < tend and nstep < nstepmax (0 for free slots)
+    int pad0;
+    unsigned long long cour[2];  // Courant maxima of the current state (bit patterns)
+    long long stop_step;         // global step at which the instance stopped (-1: running)
+};
+
+struct WorkItem {
+    int slot;
+    int dir;   // 1: x item (row, first window), 2: y item (first column, first row)
+    int line;  // x: interior row l; y: first interior column l of the 64-column group
+    int k0;    // x: first cell window; y: first output cell (row) of the segment
+};
+
+constexpr int kBatchThreads = 64;   // CTA of the batched sweep (two warps)
+constexpr int kXItemWindows = 8;    // cell windows per x item (4 per warp)
+
+struct BatchLaunch {
+    BatchInst* inst;
+    const WorkItem* items;
+    int nitems;
+    int phase;                 // 1: A -> B (first sweep of the step), 2: B -> A
+    unsigned int* counter;     // claim counter, zero before the launch
+    int seg;                   // y-segment length used to build the items
+    int claim;                 // items claimed per atomic
+};
+
+// Launchers (hb_kernels.cu for FP64, hb_mixed.cu for the mixed form).
+cudaError_t launch_batch_sweep(const BatchLaunch& L, const Phys& P, int grid, cudaStream_t s);
+cudaError_t launch_batch_sweep_mixed(const BatchLaunch& L, const Phys& P, int grid,
+                                     cudaStream_t s);
+int batch_sweep_blocks_per_sm(bool mixed, bool unit_slope);
+cudaError_t launch_batch_clock_begin(BatchInst* inst, int nslots, double courant_factor,
+                                     double smallc, long long* gstep, cudaStream_t s);
+cudaError_t launch_batch_clock_end(BatchInst* inst, int nslots, long long* gstep,
+                                   cudaStream_t s);
+// Courant maxima of the listed instances' current states (slot per entry).
+cudaError_t launch_batch_courant(BatchInst* inst, const int* slots, int nslots, const Phys& P,
+                                 cudaStream_t s);
+
+}  // namespace hb

@@ -1,0 +1,83 @@
+// hb_batch_body.cuh -- the persistent batched sweep (device side), templated
+// on the stage set.  Included by hb_kernels.cu (FP64) and hb_mixed.cu (mixed).
+#pragma once
+
+#include "hb_batch.cuh"
+#include "hb_march.cuh"
+
+namespace hb {
+
+__device__ __forceinline__ SweepArgs batch_args(const BatchInst& I, int dir, int phase,
+                                                bool fuse, BatchInst* Ip) {
+    SweepArgs a;
+    a.in = phase == 1 ? I.A : I.B;
+    a.out = phase == 1 ? I.B : I.A;
+    a.resid = I.A;
+    a.gout = I.A;
+    a.clk = nullptr;
+    a.dt = I.dt;
+    a.courant = fuse ? Ip->cour : nullptr;
+    a.nx = I.nx;
+    a.ny = I.ny;
+    a.nxt = I.nxt;
+    a.nyt = I.nyt;
+    a.vs = I.vs;
+    if (dir == 1) {
+        a.bnd_lo = I.bnd_left;
+        a.bnd_hi = I.bnd_right;
+        a.nlines = I.ny;
+        a.n = I.nxt;
+    } else {
+        a.bnd_lo = I.bnd_down;
+        a.bnd_hi = I.bnd_up;
+        a.nlines = I.nx;
+        a.n = I.nyt;
+    }
+    a.seg = 0;
+    return a;
+}
+
+// Persistent CTAs claim `claim` items at a time until the list is exhausted.
+// An item's instance is skipped once its clock has stopped.  The second
+// sweep of an instance's odd step also reduces its Courant maxima.
+template <class S>
+__device__ __forceinline__ void batch_sweep_body(const BatchLaunch& L, const Phys& P) {
+    __shared__ int s_base;
+    const typename S::Consts C = S::consts(P);
+    for (;;) {
+        if (threadIdx.x == 0) s_base = (int)atomicAdd(L.counter, (unsigned)L.claim);
+        __syncthreads();
+        const int base = s_base;
+        __syncthreads();
+        if (base >= L.nitems) break;
+        const int end = min(base + L.claim, L.nitems);
+        for (int it = base; it < end; it++) {
+            const WorkItem w = L.items[it];
+            BatchInst* Ip = L.inst + w.slot;
+            const BatchInst I = *Ip;
+            if (!I.active) continue;  // CTA-uniform
+            const bool fuse = (L.phase == 2) && (I.nstep & 1);
+            const SweepArgs a = batch_args(I, w.dir, L.phase, fuse, Ip);
+            const double dtdx = I.dt / I.dx;
+            double cx = 0.0, cy = 0.0;
+            if (w.dir == 1) {
+                const int warp = threadIdx.x >> 5;
+                for (int win = w.k0 + warp; win < w.k0 + kXItemWindows; win += kBatchThreads / 32)
+                    xcell_window<S>(a, C, w.line, win, dtdx, cx, cy);
+            } else {
+                const int l = w.line + threadIdx.x;
+                if (l < a.nlines) {
+                    const LineGeom<2> g(a, l);
+                    const int k1 = min(w.k0 + L.seg, a.n - 2);
+                    march<2, S>(a, C, g, w.k0, k1, dtdx, cx, cy);
+                }
+            }
+            if (fuse) {
+                warp_max_atomic(&Ip->cour[0], cx);
+                warp_max_atomic(&Ip->cour[1], cy);
+            }
+        }
+    }
+}
+
+}  // namespace hb

@@ -24,6 +24,7 @@
 // ends in the resident array after both sweeps.
 #include "hb_kernels.cuh"
 #include "hb_march.cuh"
+#include "hb_batch_body.cuh"
 
 namespace hb {
 
@@ -192,6 +193,104 @@ cudaError_t launch_clock_begin(DevClock* c, unsigned long long* cour, double cou
 
 cudaError_t launch_clock_end(DevClock* c, cudaStream_t s) {
     clock_end_kernel<<<1, 1, 0, s>>>(c);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- batches
+template <bool UNIT>
+__global__ void __launch_bounds__(kBatchThreads)
+batch_sweep_kernel(const BatchLaunch L, const Phys P) {
+    batch_sweep_body<ExactStages<UNIT>>(L, P);
+}
+
+cudaError_t launch_batch_sweep(const BatchLaunch& L, const Phys& P, int grid, cudaStream_t s) {
+    if (P.unit_slope) batch_sweep_kernel<true><<<grid, kBatchThreads, 0, s>>>(L, P);
+    else batch_sweep_kernel<false><<<grid, kBatchThreads, 0, s>>>(L, P);
+    return cudaGetLastError();
+}
+
+int batch_sweep_blocks_per_sm_exact(bool unit_slope) {
+    int n = 0;
+    cudaError_t e = unit_slope ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                                     &n, batch_sweep_kernel<true>, kBatchThreads, 0)
+                               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                                     &n, batch_sweep_kernel<false>, kBatchThreads, 0);
+    return (e == cudaSuccess && n > 0) ? n : 1;
+}
+
+// main.c:349-392 per instance (see clock_begin_kernel).
+__global__ void batch_clock_begin_kernel(BatchInst* inst, int nslots, double courant_factor,
+                                         double smallc, long long* gstep) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nslots) return;
+    BatchInst& I = inst[s];
+    if (!I.active) return;
+    if (!((I.t < I.tend) && (I.nstep < I.nstepmax))) {
+        I.active = 0;
+        I.stop_step = *gstep;
+        return;
+    }
+    if ((I.nstep % 2) == 0) {
+        const double cx = __longlong_as_double((long long)I.cour[0]);
+        const double cy = __longlong_as_double((long long)I.cour[1]);
+        double dt = courant_factor * I.dx / omax(cx, omax(cy, smallc));
+        if (I.nstep == 0) dt = dt / 2.0;
+        I.dt = dt;
+        I.cour[0] = 0ull;
+        I.cour[1] = 0ull;
+    }
+}
+
+__global__ void batch_clock_end_kernel(BatchInst* inst, int nslots, long long* gstep) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s == 0) *gstep += 1;
+    if (s >= nslots) return;
+    BatchInst& I = inst[s];
+    if (!I.active) return;
+    I.nstep++;
+    I.t += I.dt;
+}
+
+cudaError_t launch_batch_clock_begin(BatchInst* inst, int nslots, double courant_factor,
+                                     double smallc, long long* gstep, cudaStream_t s) {
+    batch_clock_begin_kernel<<<(nslots + 127) / 128, 128, 0, s>>>(inst, nslots, courant_factor,
+                                                                  smallc, gstep);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_clock_end(BatchInst* inst, int nslots, long long* gstep,
+                                   cudaStream_t s) {
+    batch_clock_end_kernel<<<(nslots + 127) / 128, 128, 0, s>>>(inst, nslots, gstep);
+    return cudaGetLastError();
+}
+
+// Courant maxima of the listed instances (one CTA row-stride per instance).
+__global__ void __launch_bounds__(256)
+batch_courant_kernel(BatchInst* inst, const int* slots, int nslots, Phys P) {
+    const int e = blockIdx.y;
+    if (e >= nslots) return;
+    BatchInst* Ip = inst + slots[e];
+    const BatchInst I = *Ip;
+    double cx = 0.0, cy = 0.0;
+    const long long total = (long long)I.nx * I.ny;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < total;
+         c += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(c / I.nx) + 2, i = (int)(c % I.nx) + 2;
+        const double* u = I.A + i + (long long)I.nxt * j;
+        const Cons w{u[0], u[I.vs], u[2 * I.vs], u[3 * I.vs]};
+        double cn, ct;
+        courant_speeds(P, w, cn, ct);
+        cx = omax(cx, cn);
+        cy = omax(cy, ct);
+    }
+    warp_max_atomic(&Ip->cour[0], cx);
+    warp_max_atomic(&Ip->cour[1], cy);
+}
+
+cudaError_t launch_batch_courant(BatchInst* inst, const int* slots, int nslots, const Phys& P,
+                                 cudaStream_t s) {
+    if (nslots <= 0) return cudaSuccess;
+    batch_courant_kernel<<<dim3(16, nslots), 256, 0, s>>>(inst, slots, nslots, P);
     return cudaGetLastError();
 }
 

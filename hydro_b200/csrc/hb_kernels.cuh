@@ -45,6 +45,7 @@ cudaError_t launch_sweep(int dir, const SweepArgs& a, const Phys& P, cudaStream_
 int sweep_blocks_per_sm(int dir, bool unit_slope);
 // The x sweep with one cell per lane (hb_march.cuh xcell_body): FP64 and mixed.
 constexpr int kCellThreads = 64;
+constexpr int kCellWarpOut = 28;  // outputs per warp of the cell-per-lane x sweep
 cudaError_t launch_xcell(const SweepArgs& a, const Phys& P, cudaStream_t s);
 cudaError_t launch_xcell_mixed(const SweepArgs& a, const Phys& P, cudaStream_t s);
 // The mixed-precision sweep (hb_mixed.cu).

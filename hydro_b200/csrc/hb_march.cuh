@@ -274,20 +274,54 @@ __device__ __forceinline__ F flux_up(const F& f) {
     return F{shfl_up1(f.d), shfl_up1(f.mn), shfl_up1(f.mt), shfl_up1(f.e)};
 }
 
-constexpr int kCellWarpOut = 28;  // outputs per warp of the cell-per-lane x sweep
 
-// Grid: x = rows, y = ceil(windows / warps per CTA); window = 28 output cells.
+// One warp's window: row `row`, output cells [c, c + 28) with c = 2 + 28 * win.
+// Accumulates the fused Courant maxima of its outputs into cx, cy.  The
+// caller guarantees the warp is converged and `row` < a.nlines.
 template <class S>
-__device__ __forceinline__ void xcell_body(const SweepArgs& a, const Phys& P) {
+__device__ __forceinline__ void xcell_window(const SweepArgs& a, const typename S::Consts& C,
+                                             int row, int win, double dtdx, double& cx,
+                                             double& cy) {
     using Prim = typename S::Prim;
     using Flux = typename S::Flux;
     using Real = typename S::Real;
     const int lane = threadIdx.x & 31;
-    const int warp = blockIdx.y * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    const int row = blockIdx.x;                       // interior row index l
-    const int c = 2 + warp * kCellWarpOut;            // first output cell of the warp
-    const int k = c - 2 + lane;                       // this lane's cell
-    bool active = row < a.nlines && c < a.n - 2;      // warp-uniform
+    const int c = 2 + win * kCellWarpOut;            // first output cell of the warp
+    if (c >= a.n - 2) return;                        // warp-uniform
+    const int k = c - 2 + lane;                      // this lane's cell
+    const LineGeom<1> g(a, row);
+    const typename S::TraceK K = S::trace_constants(C, dtdx);
+    const bool inside = k < a.n;                     // lanes past the row end idle
+    const Cons u = inside ? load_cell<1>(a, g, k) : Cons{1.0, 0.0, 0.0, 1.0};
+    Prim q;
+    Real cs;
+    S::prim(C, u, q, cs);
+    const Prim qm = prim_up(q), qp = prim_down(q);
+    Prim dq = S::zero_prim();
+    if (S::second_order(C)) S::slope4(C, qm, q, qp, dq);
+    Prim xm, xp;
+    S::trace(K, q, dq, cs, xm, xp);
+    const Prim xp_next = prim_down(xp);              // qxp of cell k + 1
+    const Flux f = S::riemann(C, xm, xp_next);       // interface (k | k + 1)
+    const Flux f_prev = flux_up(f);                  // interface (k - 1 | k)
+    if (lane >= 2 && lane < 2 + kCellWarpOut && k < a.n - 2) {
+        const Cons o = S::update(u, f_prev, f, dtdx);
+        store_cell<1>(a, g, k, o);
+        if (a.courant) {
+            double cn, ct;
+            S::courant(C, o, cn, ct);
+            cx = cx > cn ? cx : cn;
+            cy = cy > ct ? cy : ct;
+        }
+    }
+}
+
+// Grid: x = rows, y = ceil(windows / warps per CTA).
+template <class S>
+__device__ __forceinline__ void xcell_body(const SweepArgs& a, const Phys& P) {
+    const int win = blockIdx.y * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int row = blockIdx.x;
+    bool active = row < a.nlines;
     double dt = a.dt;
     if (a.clk) {
         active = active && a.clk->active;
@@ -296,32 +330,7 @@ __device__ __forceinline__ void xcell_body(const SweepArgs& a, const Phys& P) {
     double cx = 0.0, cy = 0.0;
     if (active) {
         const typename S::Consts C = S::consts(P);
-        const LineGeom<1> g(a, row);
-        const double dtdx = dt / P.dx;
-        const typename S::TraceK K = S::trace_constants(C, dtdx);
-        const bool inside = k < a.n;                  // lanes past the row end idle
-        const Cons u = inside ? load_cell<1>(a, g, k) : Cons{1.0, 0.0, 0.0, 1.0};
-        Prim q;
-        Real cs;
-        S::prim(C, u, q, cs);
-        const Prim qm = prim_up(q), qp = prim_down(q);
-        Prim dq = S::zero_prim();
-        if (S::second_order(C)) S::slope4(C, qm, q, qp, dq);
-        Prim xm, xp;
-        S::trace(K, q, dq, cs, xm, xp);
-        const Prim xp_next = prim_down(xp);           // qxp of cell k + 1
-        const Flux f = S::riemann(C, xm, xp_next);    // interface (k | k + 1)
-        const Flux f_prev = flux_up(f);               // interface (k - 1 | k)
-        if (lane >= 2 && lane < 2 + kCellWarpOut && k < a.n - 2) {
-            const Cons o = S::update(u, f_prev, f, dtdx);
-            store_cell<1>(a, g, k, o);
-            if (a.courant) {
-                double cn, ct;
-                S::courant(C, o, cn, ct);
-                cx = cn;
-                cy = ct;
-            }
-        }
+        xcell_window<S>(a, C, row, win, dt / P.dx, cx, cy);
     }
     if (a.courant) {
         warp_max_atomic(&a.courant[0], cx);

@@ -4,6 +4,7 @@
 #include "hb_kernels.cuh"
 #include "hb_march.cuh"
 #include "hb_stages_mixed.cuh"
+#include "hb_batch_body.cuh"
 
 namespace hb {
 
@@ -42,6 +43,27 @@ int sweep_mixed_blocks_per_sm(int dir) {
                                    &n, sweep_mixed_kernel<1>, kSweepThreads, 0)
                              : cudaOccupancyMaxActiveBlocksPerMultiprocessor(
                                    &n, sweep_mixed_kernel<2>, kSweepThreads, 0);
+    return (e == cudaSuccess && n > 0) ? n : 1;
+}
+
+__global__ void __launch_bounds__(kBatchThreads)
+batch_sweep_mixed_kernel(const BatchLaunch L, const Phys P) {
+    batch_sweep_body<MixedStages>(L, P);
+}
+
+cudaError_t launch_batch_sweep_mixed(const BatchLaunch& L, const Phys& P, int grid,
+                                     cudaStream_t s) {
+    batch_sweep_mixed_kernel<<<grid, kBatchThreads, 0, s>>>(L, P);
+    return cudaGetLastError();
+}
+
+int batch_sweep_blocks_per_sm_exact(bool unit_slope);  // hb_kernels.cu
+
+int batch_sweep_blocks_per_sm(bool mixed, bool unit_slope) {
+    if (!mixed) return batch_sweep_blocks_per_sm_exact(unit_slope);
+    int n = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_sweep_mixed_kernel,
+                                                                  kBatchThreads, 0);
     return (e == cudaSuccess && n > 0) ? n : 1;
 }
 

@@ -211,6 +211,47 @@ int hydro_b200_domain_profile_read(hb_domain *d, double *ms, long long *count, i
 /* Number of kernel launches the library issued on this domain so far. */
 long long hydro_b200_domain_launch_count(hb_domain *d);
 
+/* ------------------------------------------------------------------------
+ * Batches: many independent runs of different grid sizes advanced together.
+ * One global step advances every active instance by one time step of its own
+ * (its own dt, main.c:344-408 semantics per instance) with two persistent
+ * launches that pull work items of all instances from a queue; each step is
+ * replayed as a CUDA graph.  Instance states live in one device arena.
+ * ------------------------------------------------------------------------ */
+typedef struct hb_batch hb_batch;
+/* H supplies the constants shared by every instance (gamma, smallr, smallc,
+ * courant_factor, niter_riemann, iorder, slope_type, scheme); capacity is the
+ * number of slots, arena_bytes the device memory for states and scratch. */
+hb_batch *hydro_b200_batch_create(const hydroparam_t *H, int capacity, size_t arena_bytes,
+                                  int precision);
+void hydro_b200_batch_destroy(hb_batch *b);
+/* Device bytes an instance of grid H takes in the arena. */
+long long hydro_b200_batch_bytes_needed(const hydroparam_t *H);
+long long hydro_b200_batch_arena_free(hb_batch *b);
+/* Admit an instance (grid nx, ny, dx and boundary types from H, clock from
+ * H->t and H->nstep, state from host memory in the reference layout); it runs
+ * until t >= tend or nstep >= nstepmax.  Returns its slot, or -1 when no slot
+ * or arena space is free (HB_ERR_NOMEM). */
+int hydro_b200_batch_add(hb_batch *b, const hydroparam_t *H, const double *host, double tend,
+                         int nstepmax);
+int hydro_b200_batch_remove(hb_batch *b, int slot);
+int hydro_b200_batch_steps(hb_batch *b, int nsteps); /* asynchronous */
+int hydro_b200_batch_synchronize(hb_batch *b);
+int hydro_b200_batch_status(hb_batch *b, int slot, double *t, int *nstep, double *dt, int *active,
+                            long long *stop_step);
+int hydro_b200_batch_poll(hb_batch *b, int *active, int n);
+int hydro_b200_batch_download(hb_batch *b, int slot, double *host);
+long long hydro_b200_batch_global_step(hb_batch *b);
+long long hydro_b200_batch_launch_count(hb_batch *b);
+void *hydro_b200_batch_stream(hb_batch *b);
+/* Tiling of the work items: y-segment length, items per queue claim,
+ * persistent CTAs per SM (0 = occupancy limit).  Results do not depend on it. */
+int hydro_b200_batch_set_tuning(hb_batch *b, int seg, int claim, int blocks_per_sm);
+int hydro_b200_batch_get_tuning(hb_batch *b, int *seg, int *claim, int *blocks_per_sm);
+/* Times `steps` real global steps per candidate tiling and keeps the fastest
+ * (cached per mix of grid shapes).  Returns the global steps advanced. */
+int hydro_b200_batch_autotune(hb_batch *b, int steps);
+
 /* Select the CUDA device used by the calling thread for domains and mirrors
  * created afterwards (the library links its own CUDA runtime, so a device
  * chosen through another runtime instance does not carry over). */
