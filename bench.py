@@ -177,6 +177,67 @@ def dom_state_after(H, u0, nsteps, precision):
     return u
 
 
+def run_batched_form(device, seed=20261203, n=256, nsteps=100):
+    """The batched workload: n seeded instances (sides log-uniform in
+    [64, 1024], multiples of 8), mixed precision, nsteps steps each, one
+    persistent launch per sweep, CUDA graphs, autotuned tiles (tuned on a
+    throwaway batch of the same mix, then timed on a fresh one)."""
+    import torch
+    from hydro_b200 import Batch, make_blast_mix
+    mix = make_blast_mix(n, seed)
+    H0 = mix[0][0]
+    arena = sum(Batch.bytes_needed(H) for H, _ in mix) + (1 << 20)
+    tb = Batch(H0, n, arena, precision="mixed")
+    for H, u in mix:
+        tb.add(H, u, nstepmax=nsteps)
+    tb.autotune(steps=1)
+    tuning = tb.tuning()
+    tb.close()
+    b = Batch(H0, n, arena, precision="mixed")
+    slots = [b.add(H, u, nstepmax=nsteps) for H, u in mix]
+    b.autotune(steps=1)  # cache hit: applies the tuning without stepping
+    b.steps(0)
+    b.synchronize()
+    st = torch.cuda.ExternalStream(b.stream_ptr, device=device)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = b.launch_count
+    e0.record(st)
+    b.steps(nsteps)
+    e1.record(st)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    active, nstep, _ = b.table()
+    done = int(sum(1 for s in slots if nstep[s] == nsteps))
+    cells = sum(H.nx * H.ny for H, _ in mix)
+    launches = b.launch_count - l0
+    b.close()
+    return {"workload": f"{n} seeded blast instances, sides 64..1024, {nsteps} steps each",
+            "value": round(cells * nsteps / (ms / 1e3) / 1e6, 3), "unit": "Mcell-updates/s",
+            "ms": round(ms, 3), "instances_finished": done, "cells": cells,
+            "graph_launches": nsteps, "kernel_launches": launches, "tuning": tuning,
+            "precision": "mixed"}
+
+
+def run_serving_form(label, rate, n, side_lo, side_hi, tend_lo, tend_hi, wall_s, seed=20261204):
+    """The serving loop (continuous batching) on a Poisson request stream;
+    arena = 80% of the free HBM; time-bounded."""
+    import torch
+    from hydro_b200 import make_params
+    from hydro_b200.serve import BatchBackend, Server, poisson_requests
+    free, total = torch.cuda.mem_get_info()
+    budget = int(0.8 * free)
+    reqs = poisson_requests(n, rate, seed, side_lo, side_hi, tend_lo, tend_hi)
+    be = BatchBackend(make_params(128, 128), budget, capacity=4096)
+    st = Server(be).run(reqs, max_wall_s=wall_s)
+    be.close()
+    out = st.summary()
+    out.update({"label": label, "lambda_per_s": rate, "requests_offered": n,
+                "sides": [side_lo, side_hi], "tend": [tend_lo, tend_hi],
+                "hbm_budget_gb": round(budget / 1e9, 1), "wall_limit_s": wall_s,
+                "precision": "mixed"})
+    return out
+
+
 def cpu_reference_sample(wl, budget_s, max_steps, warm=1):
     """The reference's own C99/OpenMP code (oracle/_ref) on the host cores,
     falling back to the C restatement (oracle/_build) where the reference was
@@ -244,6 +305,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--serving-wall", type=float, default=25.0)
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
     if args.warmup < 3:
@@ -347,6 +411,16 @@ def main():
                           "errors_vs_fp64": err,
                           "precision": "FP32 stages; FP64 Newton p*, update, Courant"}
         del ref_state, mix_state
+
+    if not args.no_batched and rank == 0:
+        forms["batched"] = run_batched_form(device)
+    if not args.no_serving and rank == 0:
+        forms["serving"] = run_serving_form(
+            "configured stream: lambda 200/s, sides 128..4096, tend 0.01..0.1 (time-bounded)",
+            200.0, 10000, 128, 4096, 0.01, 0.1, args.serving_wall)
+        forms["serving_subsaturating"] = run_serving_form(
+            "sub-saturating stream (labelled): lambda 20/s, sides 128..512, tend 0.01..0.03",
+            20.0, 400, 128, 512, 0.01, 0.03, args.serving_wall)
 
     # End to end through the reference entry points on a pinned host array.
     e2e = None

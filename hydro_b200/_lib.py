@@ -135,12 +135,16 @@ SIGNATURES = [
     ("hydro_b200_batch_bytes_needed", C.c_longlong, [_P]),
     ("hydro_b200_batch_arena_free", C.c_longlong, [_D]),
     ("hydro_b200_batch_add", C.c_int, [_D, _P, C.c_void_p, C.c_double, C.c_int]),
+    ("hydro_b200_batch_add_blast", C.c_int, [_D, _P, C.c_double, C.c_double, C.c_int, C.c_int,
+                                             C.c_double, C.c_double, C.c_int]),
     ("hydro_b200_batch_remove", C.c_int, [_D, C.c_int]),
     ("hydro_b200_batch_steps", C.c_int, [_D, C.c_int]),
     ("hydro_b200_batch_synchronize", C.c_int, [_D]),
     ("hydro_b200_batch_status", C.c_int, [_D, C.c_int, _DP, C.POINTER(C.c_int), _DP,
                                           C.POINTER(C.c_int), C.POINTER(C.c_longlong)]),
     ("hydro_b200_batch_poll", C.c_int, [_D, C.POINTER(C.c_int), C.c_int]),
+    ("hydro_b200_batch_table", C.c_int, [_D, C.POINTER(C.c_int), C.POINTER(C.c_int), _DP,
+                                         C.c_int]),
     ("hydro_b200_batch_download", C.c_int, [_D, C.c_int, C.c_void_p]),
     ("hydro_b200_batch_global_step", C.c_longlong, [_D]),
     ("hydro_b200_batch_launch_count", C.c_longlong, [_D]),

@@ -67,6 +67,22 @@ class Batch:
         self.params[slot] = H
         return slot
 
+    def try_add_blast(self, H: HydroParam, rho: float, e_bg: float, cell: tuple, e_blast: float,
+                      tend: float = 1e300, nstepmax: int = 2**31 - 1) -> int:
+        """Admit a single-blast instance generated on the device; `cell` is
+        the padded (i, j) of the blast.  Returns the slot, or -1 when full."""
+        slot = self.lib.hydro_b200_batch_add_blast(self.h, C.byref(H), rho, e_bg, int(cell[0]),
+                                                   int(cell[1]), e_blast, tend, nstepmax)
+        if slot < 0:
+            err = self.lib.hydro_b200_last_error()
+            msg = self.lib.hydro_b200_last_error_message().decode(errors="replace")
+            self.lib.hydro_b200_clear_error()
+            if err != _lib.HB_ERR_NOMEM:
+                raise _lib.HydroB200Error(f"batch add failed ({err}): {msg}")
+            return -1
+        self.params[slot] = H
+        return slot
+
     def remove(self, slot: int) -> None:
         check(self.lib.hydro_b200_batch_remove(self.h, slot))
         self.params.pop(slot, None)
@@ -88,6 +104,15 @@ class Batch:
         out = (C.c_int * self.capacity)()
         check(self.lib.hydro_b200_batch_poll(self.h, out, self.capacity))
         return np.frombuffer(out, dtype=np.int32).copy()
+
+    def table(self):
+        """(active, nstep, t) arrays over all slots, one device read."""
+        a = (C.c_int * self.capacity)()
+        n = (C.c_int * self.capacity)()
+        t = (C.c_double * self.capacity)()
+        check(self.lib.hydro_b200_batch_table(self.h, a, n, t, self.capacity))
+        return (np.frombuffer(a, dtype=np.int32).copy(), np.frombuffer(n, dtype=np.int32).copy(),
+                np.frombuffer(t, dtype=np.float64).copy())
 
     def download(self, slot: int) -> np.ndarray:
         H = self.params[slot]
@@ -133,18 +158,33 @@ def _u01(seed: int, stream: int, idx: np.ndarray) -> np.ndarray:
     return (z >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
 
 
-def blast_instance(nx: int, ny: int, bx: float, by: float, e0: float, rho: float):
-    """A single-blast instance: density rho, u = v = 0, E = 1e-5, and
-    E = e0/dx^2 in the cell at fractional position (bx, by) of the interior;
-    dx = 1/nx, reflecting walls."""
+E_BACKGROUND = 1e-5
+
+
+def blast_spec(nx: int, ny: int, bx: float, by: float, e0: float, rho: float):
+    """Parameters of a single-blast instance: density rho, u = v = 0,
+    E = 1e-5, and E = e0/dx^2 in the cell at fractional position (bx, by) of
+    the interior; dx = 1/nx, reflecting walls.  Returns (H, rho, e_bg,
+    (i, j) padded blast cell, e_blast)."""
     H = make_params(nx, ny, testcase=0)
-    u = np.zeros(state_shape(H), dtype=np.float64)
-    u[0, 2:-2, 2:-2] = rho
-    u[3, 2:-2, 2:-2] = 1e-5
     i = 2 + min(int(bx * nx), nx - 1)
     j = 2 + min(int(by * ny), ny - 1)
-    u[3, j, i] = e0 / H.dx / H.dx
-    return H, u
+    return H, rho, E_BACKGROUND, (i, j), e0 / H.dx / H.dx
+
+
+def blast_state(H: HydroParam, rho: float, e_bg: float, cell: tuple, e_blast: float):
+    """The host array of blast_spec's instance (what the device init writes)."""
+    u = np.zeros(state_shape(H), dtype=np.float64)
+    u[0, 2:-2, 2:-2] = rho
+    u[3, 2:-2, 2:-2] = e_bg
+    u[3, cell[1], cell[0]] = e_blast
+    return u
+
+
+def blast_instance(nx: int, ny: int, bx: float, by: float, e0: float, rho: float):
+    """blast_spec's instance as (H, host state)."""
+    H, rho, e_bg, cell, eb = blast_spec(nx, ny, bx, by, e0, rho)
+    return H, blast_state(H, rho, e_bg, cell, eb)
 
 
 def make_blast_mix(n: int, seed: int, side_lo: int = 64, side_hi: int = 1024,

@@ -441,6 +441,57 @@ extern "C" int hydro_b200_batch_add(hb_batch* b, const hydroparam_t* H, const do
     return slot;
 }
 
+// Admit an instance whose initial state is a single blast written on the
+// device (no host state): density rho, energy e_bg, and e_blast in the
+// padded cell (bi, bj).
+extern "C" int hydro_b200_batch_add_blast(hb_batch* b, const hydroparam_t* H, double rho,
+                                          double e_bg, int bi, int bj, double e_blast, double tend,
+                                          int nstepmax) {
+    if (!b || !H) return fail(HB_ERR_ARG, "add_blast: null argument"), -1;
+    if (H->nx < 3 || H->ny < 3 || bi < 2 || bi >= H->nx + 2 || bj < 2 || bj >= H->ny + 2)
+        return fail(HB_ERR_ARG, "add_blast: blast cell outside the interior"), -1;
+    if (sync_table_down(b) != HB_OK) return -1;
+    int slot = -1;
+    for (int s = 0; s < b->capacity; s++)
+        if (b->off[s] < 0) {
+            slot = s;
+            break;
+        }
+    if (slot < 0) return fail(HB_ERR_NOMEM, "add: no free slot"), -1;
+    const long long u = units_for(H);
+    const long long o = b->arena.alloc(2 * u);
+    if (o < 0) return fail(HB_ERR_NOMEM, "add: arena full"), -1;
+    BatchInst I;
+    memset(&I, 0, sizeof(I));
+    I.A = b->arena.base + o * 32;
+    I.B = I.A + u * 32;
+    I.nx = H->nx;
+    I.ny = H->ny;
+    I.nxt = H->nx + 4;
+    I.nyt = H->ny + 4;
+    I.vs = (long long)I.nxt * I.nyt;
+    I.bnd_left = H->boundary_left;
+    I.bnd_right = H->boundary_right;
+    I.bnd_down = H->boundary_down;
+    I.bnd_up = H->boundary_up;
+    I.dx = H->dx;
+    I.t = H->t;
+    I.tend = tend;
+    I.nstep = H->nstep;
+    I.nstepmax = nstepmax;
+    I.active = 1;
+    I.stop_step = -1;
+    HB_BCU(hb::launch_blast_init(I.A, H->nx, H->ny, rho, e_bg, bi, bj, e_blast, b->stream));
+    b->launches += 1;
+    b->h[slot] = I;
+    b->off[slot] = o;
+    b->len[slot] = 2 * u;
+    b->table_dirty = true;
+    b->lists_dirty = true;
+    if (I.nstep % 2 == 0) b->fresh.push_back(slot);
+    return slot;
+}
+
 extern "C" int hydro_b200_batch_remove(hb_batch* b, int slot) {
     if (!b || slot < 0 || slot >= b->capacity || b->off[slot] < 0)
         return fail(HB_ERR_ARG, "remove: no such slot");
@@ -497,6 +548,21 @@ extern "C" int hydro_b200_batch_poll(hb_batch* b, int* active, int n) {
     int rc = sync_table_down(b);
     if (rc) return rc;
     for (int s = 0; s < n && s < b->capacity; s++) active[s] = b->off[s] >= 0 && b->h[s].active;
+    return HB_OK;
+}
+
+// Clocks of the first n slots in one read: active (1 running; 0 stopped or
+// free), nstep and t.
+extern "C" int hydro_b200_batch_table(hb_batch* b, int* active, int* nstep, double* t, int n) {
+    if (!b) return fail(HB_ERR_ARG, "table: null batch");
+    int rc = sync_table_down(b);
+    if (rc) return rc;
+    for (int s = 0; s < n && s < b->capacity; s++) {
+        const bool used = b->off[s] >= 0;
+        if (active) active[s] = used && b->h[s].active;
+        if (nstep) nstep[s] = used ? b->h[s].nstep : 0;
+        if (t) t[s] = used ? b->h[s].t : 0.0;
+    }
     return HB_OK;
 }
 

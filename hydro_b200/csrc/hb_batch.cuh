@@ -62,6 +62,8 @@ cudaError_t launch_batch_clock_begin(BatchInst* inst, int nslots, double courant
                                      double smallc, long long* gstep, cudaStream_t s);
 cudaError_t launch_batch_clock_end(BatchInst* inst, int nslots, long long* gstep,
                                    cudaStream_t s);
+cudaError_t launch_blast_init(double* u, int nx, int ny, double rho, double ebg, int bi, int bj,
+                              double eblast, cudaStream_t s);
 // Courant maxima of the listed instances' current states (slot per entry).
 cudaError_t launch_batch_courant(BatchInst* inst, const int* slots, int nslots, const Phys& P,
                                  cudaStream_t s);

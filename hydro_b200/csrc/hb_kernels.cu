@@ -287,6 +287,33 @@ batch_courant_kernel(BatchInst* inst, const int* slots, int nslots, Phys P) {
     warp_max_atomic(&Ip->cour[1], cy);
 }
 
+// A single-blast initial state written on the device: density rho, zero
+// momenta and energy e_bg in the interior, ghost cells 0, and energy e_blast
+// in the padded cell (bi, bj) -- the layout of hydro_funcs.c:15-112.
+__global__ void blast_init_kernel(double* u, int nx, int ny, double rho, double ebg, int bi,
+                                  int bj, double eblast) {
+    const int nxt = nx + 4, nyt = ny + 4;
+    const long long vs = (long long)nxt * nyt;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < vs;
+         c += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(c / nxt), i = (int)(c % nxt);
+        const bool in = i >= 2 && i < nx + 2 && j >= 2 && j < ny + 2;
+        u[c] = in ? rho : 0.0;
+        u[c + vs] = 0.0;
+        u[c + 2 * vs] = 0.0;
+        u[c + 3 * vs] = in ? ((i == bi && j == bj) ? eblast : ebg) : 0.0;
+    }
+}
+
+cudaError_t launch_blast_init(double* u, int nx, int ny, double rho, double ebg, int bi, int bj,
+                              double eblast, cudaStream_t s) {
+    const long long vs = (long long)(nx + 4) * (ny + 4);
+    long long blocks = (vs + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    blast_init_kernel<<<(unsigned)blocks, 256, 0, s>>>(u, nx, ny, rho, ebg, bi, bj, eblast);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_batch_courant(BatchInst* inst, const int* slots, int nslots, const Phys& P,
                                  cudaStream_t s) {
     if (nslots <= 0) return cudaSuccess;

@@ -1,0 +1,180 @@
+"""Serving loop: continuous batching of HydroC solve requests.
+
+Requests (a square grid with a single blast and an end time) arrive by a
+Poisson process.  The loop admits them first-come first-served into a batch
+(hb_batch) while their resident state fits the HBM budget, advances every
+admitted solve together -- each with its own dt -- in chunks of global steps,
+and retires solves as their clocks pass tend, which frees slots and memory
+for the queue.  Time to solution is measured from arrival (so it includes
+queueing) to the poll that sees the solve finished.
+
+The loop talks to a backend (``BatchBackend`` for the GPU); the bookkeeping
+is independent of it, so it is tested on the CPU with a simulated backend.
+"""
+from __future__ import annotations
+
+import math
+import time
+from collections import deque
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .batch import Batch, blast_spec, _u01
+
+
+@dataclass
+class Request:
+    rid: int
+    arrival: float   # seconds after the start of the stream
+    side: int        # square grid side (nx = ny)
+    tend: float
+    bx: float
+    by: float
+    e0: float
+    rho: float
+
+    @property
+    def cells(self) -> int:
+        return self.side * self.side
+
+
+def poisson_requests(n: int, rate: float, seed: int, side_lo: int = 128, side_hi: int = 4096,
+                     tend_lo: float = 0.01, tend_hi: float = 0.1) -> list:
+    """n requests: exponential inter-arrival times of mean 1/rate; square side
+    log-uniform in [side_lo, side_hi] rounded to a multiple of 8; tend
+    uniform in [tend_lo, tend_hi]; blast as in the batched workload (cell
+    uniform, E0 log-uniform in [0.1, 10]/dx^2, density uniform in [0.5, 2]).
+    Draws are SplitMix64 of (seed, stream, request index)."""
+    idx = np.arange(n, dtype=np.uint64)
+    gaps = -np.log1p(-_u01(seed, 11, idx)) / rate
+    arrivals = np.cumsum(gaps)
+    lo, hi = math.log(side_lo), math.log(side_hi)
+    sides = np.clip(np.rint(np.exp(lo + (hi - lo) * _u01(seed, 12, idx)) / 8) * 8, side_lo,
+                    side_hi).astype(int)
+    tends = tend_lo + (tend_hi - tend_lo) * _u01(seed, 13, idx)
+    bx, by = _u01(seed, 14, idx), _u01(seed, 15, idx)
+    e0 = np.exp(math.log(0.1) + (math.log(10.0) - math.log(0.1)) * _u01(seed, 16, idx))
+    rho = 0.5 + 1.5 * _u01(seed, 17, idx)
+    return [Request(int(k), float(arrivals[k]), int(sides[k]), float(tends[k]), float(bx[k]),
+                    float(by[k]), float(e0[k]), float(rho[k])) for k in range(n)]
+
+
+class BatchBackend:
+    """GPU backend: one hb_batch whose arena is the HBM budget."""
+
+    def __init__(self, H, budget_bytes: int, capacity: int = 1024, precision: str = "mixed",
+                 keep_results: bool = False):
+        self.batch = Batch(H, capacity, budget_bytes, precision=precision)
+        self.capacity = capacity
+        self.keep_results = keep_results
+        self.results = {}
+
+    def try_admit(self, req: Request) -> int:
+        H, rho, e_bg, cell, e_blast = blast_spec(req.side, req.side, req.bx, req.by, req.e0,
+                                                 req.rho)
+        return self.batch.try_add_blast(H, rho, e_bg, cell, e_blast, tend=req.tend)
+
+    def steps(self, k: int) -> None:
+        self.batch.steps(k)
+
+    def table(self):
+        return self.batch.table()
+
+    def release(self, slot: int, req: Request) -> None:
+        if self.keep_results:
+            self.results[req.rid] = self.batch.download(slot)
+        self.batch.remove(slot)
+
+    def close(self) -> None:
+        self.batch.close()
+
+
+@dataclass
+class ServeStats:
+    completed: list = field(default_factory=list)   # (rid, latency s, steps, cells)
+    admitted: int = 0
+    arrived: int = 0
+    wall_s: float = 0.0
+    cell_steps: float = 0.0
+    queue_samples: list = field(default_factory=list)  # (time s, queued, running)
+    chunks: int = 0
+    unfinished: int = 0
+
+    def summary(self) -> dict:
+        lat = np.array([c[1] for c in self.completed]) if self.completed else np.zeros(0)
+        q = [s[1] for s in self.queue_samples]
+        return {
+            "arrived": self.arrived, "admitted": self.admitted,
+            "completed": len(self.completed),
+            "wall_s": round(self.wall_s, 3),
+            "mcell_updates_per_s": round(self.cell_steps / max(self.wall_s, 1e-9) / 1e6, 3),
+            "p50_s": round(float(np.percentile(lat, 50)), 4) if lat.size else None,
+            "p99_s": round(float(np.percentile(lat, 99)), 4) if lat.size else None,
+            "queue_max": max(q) if q else 0,
+            "queue_end": q[-1] if q else 0,
+            "running_end": self.unfinished,
+            "chunks": self.chunks,
+        }
+
+
+class Server:
+    """First-come first-served continuous batching over a backend."""
+
+    def __init__(self, backend, chunk_target_s: float = 0.01, max_chunk: int = 256,
+                 clock=time.perf_counter, sleep=time.sleep):
+        self.backend = backend
+        self.chunk_target_s = chunk_target_s
+        self.max_chunk = max_chunk
+        self.clock = clock
+        self.sleep = sleep
+
+    def run(self, requests: list, max_wall_s: float) -> ServeStats:
+        st = ServeStats()
+        pending = deque(sorted(requests, key=lambda r: r.arrival))
+        queue: deque = deque()
+        running = {}          # slot -> (request, steps already counted)
+        k = 1
+        t0 = self.clock()
+        while True:
+            now = self.clock() - t0
+            if now >= max_wall_s or not (pending or queue or running):
+                break
+            while pending and pending[0].arrival <= now:
+                queue.append(pending.popleft())
+                st.arrived += 1
+            while queue:
+                slot = self.backend.try_admit(queue[0])
+                if slot < 0:
+                    break
+                running[slot] = (queue.popleft(), 0)
+                st.admitted += 1
+            st.queue_samples.append((now, len(queue), len(running)))
+            if not running:
+                if pending:
+                    self.sleep(max(0.0, min(pending[0].arrival - now, max_wall_s - now)))
+                continue
+            c0 = self.clock()
+            self.backend.steps(k)
+            active, nstep, _ = self.backend.table()
+            dtc = self.clock() - c0
+            st.chunks += 1
+            done_time = self.clock() - t0
+            for slot in list(running):
+                req, counted = running[slot]
+                n = int(nstep[slot])
+                st.cell_steps += float(req.cells) * (n - counted)
+                running[slot] = (req, n)
+                if not active[slot]:
+                    st.completed.append((req.rid, done_time - req.arrival, n, req.cells))
+                    self.backend.release(slot, req)
+                    del running[slot]
+            # Next chunk: about chunk_target_s of device work.
+            if dtc > 0:
+                k = int(max(1, min(self.max_chunk, round(k * self.chunk_target_s / dtc))))
+        st.wall_s = self.clock() - t0
+        arrived_waiting = len(queue) + sum(1 for r in pending if r.arrival <= st.wall_s)
+        st.arrived += sum(1 for r in pending if r.arrival <= st.wall_s)
+        st.queue_samples.append((st.wall_s, arrived_waiting, len(running)))
+        st.unfinished = len(running)
+        return st

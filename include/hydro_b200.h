@@ -234,12 +234,19 @@ long long hydro_b200_batch_arena_free(hb_batch *b);
  * or arena space is free (HB_ERR_NOMEM). */
 int hydro_b200_batch_add(hb_batch *b, const hydroparam_t *H, const double *host, double tend,
                          int nstepmax);
+/* The same with the initial state written on the device: a single blast
+ * (density rho, zero momenta, energy e_bg, and e_blast in the padded cell
+ * (bi, bj); ghost cells 0). */
+int hydro_b200_batch_add_blast(hb_batch *b, const hydroparam_t *H, double rho, double e_bg,
+                               int bi, int bj, double e_blast, double tend, int nstepmax);
 int hydro_b200_batch_remove(hb_batch *b, int slot);
 int hydro_b200_batch_steps(hb_batch *b, int nsteps); /* asynchronous */
 int hydro_b200_batch_synchronize(hb_batch *b);
 int hydro_b200_batch_status(hb_batch *b, int slot, double *t, int *nstep, double *dt, int *active,
                             long long *stop_step);
 int hydro_b200_batch_poll(hb_batch *b, int *active, int n);
+/* active / nstep / t of the first n slots in one read (any pointer may be NULL). */
+int hydro_b200_batch_table(hb_batch *b, int *active, int *nstep, double *t, int n);
 int hydro_b200_batch_download(hb_batch *b, int slot, double *host);
 long long hydro_b200_batch_global_step(hb_batch *b);
 long long hydro_b200_batch_launch_count(hb_batch *b);

@@ -1,0 +1,124 @@
+"""Serving-loop bookkeeping on the CPU: a simulated backend with a memory
+budget, per-request step counts and a per-cell-step cost, driven by a fake
+clock.  Checks FIFO admission under the budget, completion and latency
+accounting, work accounting, and queue growth under overload."""
+import math
+
+import pytest
+
+from hydro_b200.serve import Request, Server, poisson_requests
+
+
+class FakeClock:
+    def __init__(self):
+        self.t = 0.0
+
+    def __call__(self):
+        return self.t
+
+    def sleep(self, dt):
+        self.t += max(dt, 1e-6)
+
+
+class SimBackend:
+    """Slots with a byte budget (64 B per cell); a request needs
+    steps(side, tend) steps; a global step costs sum(cells) * cost s."""
+
+    def __init__(self, clock, budget_cells, cost=1e-9, capacity=64):
+        self.clock = clock
+        self.budget = budget_cells
+        self.cost = cost
+        self.capacity = capacity
+        self.slots = {}
+        self.admitted_order = []
+        self.peak = 0
+
+    @staticmethod
+    def steps_needed(req):
+        return max(1, int(req.side * req.tend * 4))
+
+    def used(self):
+        return sum(r.cells for r, _ in self.slots.values())
+
+    def try_admit(self, req):
+        if len(self.slots) >= self.capacity or self.used() + req.cells > self.budget:
+            return -1
+        slot = min(set(range(self.capacity)) - set(self.slots))
+        self.slots[slot] = (req, 0)
+        self.admitted_order.append(req.rid)
+        self.peak = max(self.peak, self.used())
+        return slot
+
+    def steps(self, k):
+        for _ in range(k):
+            cells = 0
+            for s, (r, n) in list(self.slots.items()):
+                if n < self.steps_needed(r):
+                    self.slots[s] = (r, n + 1)
+                    cells += r.cells
+            self.clock.t += cells * self.cost
+
+    def table(self):
+        active = [0] * self.capacity
+        nstep = [0] * self.capacity
+        for s, (r, n) in self.slots.items():
+            active[s] = int(n < self.steps_needed(r))
+            nstep[s] = n
+        return active, nstep, [0.0] * self.capacity
+
+    def release(self, slot, req):
+        del self.slots[slot]
+
+
+def test_poisson_requests_are_seeded_and_in_range():
+    a = poisson_requests(2000, 200.0, seed=4)
+    b = poisson_requests(2000, 200.0, seed=4)
+    assert [r.__dict__ for r in a] == [r.__dict__ for r in b]
+    assert all(128 <= r.side <= 4096 and r.side % 8 == 0 for r in a)
+    assert all(0.01 <= r.tend <= 0.1 for r in a)
+    gaps = [a[i + 1].arrival - a[i].arrival for i in range(len(a) - 1)]
+    mean = sum(gaps) / len(gaps)
+    assert abs(mean - 1 / 200.0) < 0.1 / 200.0
+    logs = [math.log(r.side) for r in a]
+    assert abs(sum(logs) / len(logs) - (math.log(128) + math.log(4096)) / 2) < 0.1
+
+
+def test_light_load_completes_everything_fifo():
+    clk = FakeClock()
+    be = SimBackend(clk, budget_cells=10**6)
+    reqs = poisson_requests(40, 5.0, seed=1, side_lo=32, side_hi=128)
+    st = Server(be, clock=clk, sleep=clk.sleep).run(reqs, max_wall_s=1e6)
+    assert len(st.completed) == 40 and st.admitted == 40
+    assert be.admitted_order == sorted(be.admitted_order)
+    by_id = {r.rid: r for r in reqs}
+    work = sum(r.cells * SimBackend.steps_needed(r) for r in reqs)
+    assert st.cell_steps == work
+    for rid, lat, n, cells in st.completed:
+        assert n == SimBackend.steps_needed(by_id[rid]) and lat > 0
+    s = st.summary()
+    assert s["completed"] == 40 and s["p50_s"] <= s["p99_s"]
+
+
+def test_budget_is_never_exceeded_and_overload_queues():
+    clk = FakeClock()
+    budget = 3 * 128 * 128
+    be = SimBackend(clk, budget_cells=budget, cost=1e-7)
+    reqs = poisson_requests(300, 500.0, seed=2, side_lo=64, side_hi=128)
+    st = Server(be, clock=clk, sleep=clk.sleep).run(reqs, max_wall_s=0.5)
+    assert be.peak <= budget
+    s = st.summary()
+    assert s["queue_end"] > 0 and s["completed"] < 300
+    assert st.admitted == s["completed"] + s["running_end"]
+
+
+def test_head_of_line_waits_for_memory():
+    """A request larger than the free budget waits; later small ones do not
+    overtake it (first-come first-served)."""
+    clk = FakeClock()
+    be = SimBackend(clk, budget_cells=2 * 100 * 100, cost=1e-6)
+    reqs = [Request(1, 0.0, 100, 0.05, .5, .5, 1., 1.),      # fits
+            Request(3, 0.0005, 120, 0.05, .5, .5, 1., 1.),   # must wait for memory
+            Request(2, 0.001, 8, 0.01, .5, .5, 1., 1.)]      # small, arrives last
+    st = Server(be, clock=clk, sleep=clk.sleep).run(reqs, max_wall_s=1e3)
+    assert be.admitted_order == [1, 3, 2]
+    assert len(st.completed) == 3
