@@ -180,7 +180,7 @@ int build_lists(hb_batch* b) {
                     for (int k0 = 2; k0 < I.ny + 2; k0 += b->tune.seg)
                         L[list].push_back(WorkItem{s, 2, l0, k0});
             } else {
-                const int nwin = (I.nx + hb::kCellWarpOut - 1) / hb::kCellWarpOut;
+                const int nwin = (I.nx + 2 + hb::kCellWarpOut - 1) / hb::kCellWarpOut;
                 for (int l = 0; l < I.ny; l++)
                     for (int w0 = 0; w0 < nwin; w0 += hb::kXItemWindows)
                         L[list].push_back(WorkItem{s, 1, l, w0});

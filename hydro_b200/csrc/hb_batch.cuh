@@ -29,7 +29,11 @@ struct BatchInst {
     int nstep, nstepmax;
     int active;         // 1 while t < tend and nstep < nstepmax (0 for free slots)
     int pad0;
-    unsigned long long cour[2];  // Courant maxima of the current state (bit patterns)
+    // Courant maxima of the current state (bit patterns): kBatchCourSlots slots
+    // of max(c+|u|) then kBatchCourSlots of max(c+|v|), the slot chosen by the
+    // CTA, so that large instances do not funnel every warp's atomic into one
+    // address; readers take the max over the slots.
+    unsigned long long cour[2 * 16];
     long long stop_step;         // global step at which the instance stopped (-1: running)
 };
 
@@ -41,6 +45,7 @@ struct WorkItem {
 };
 
 constexpr int kBatchThreads = 64;   // CTA of the batched sweep (two warps)
+constexpr int kBatchCourSlots = 16; // Courant accumulator slots per instance
 constexpr int kXItemWindows = 8;    // cell windows per x item (4 per warp)
 
 struct BatchLaunch {

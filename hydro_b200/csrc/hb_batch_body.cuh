@@ -73,8 +73,9 @@ __device__ __forceinline__ void batch_sweep_body(const BatchLaunch& L, const Phy
                 }
             }
             if (fuse) {
-                warp_max_atomic(&Ip->cour[0], cx);
-                warp_max_atomic(&Ip->cour[1], cy);
+                const int slot = blockIdx.x % kBatchCourSlots;
+                warp_max_atomic(&Ip->cour[slot], cx);
+                warp_max_atomic(&Ip->cour[kBatchCourSlots + slot], cy);
             }
         }
     }

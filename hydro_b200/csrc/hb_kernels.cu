@@ -41,7 +41,8 @@ xcell_kernel(const SweepArgs a, const Phys P) {
 }
 
 static dim3 xcell_grid(const SweepArgs& a) {
-    const int nwin = (a.n - 4 + kCellWarpOut - 1) / kCellWarpOut;
+    // Windows [28w, 28w + 28) cover the outputs [2, n - 2).
+    const int nwin = (a.n - 2 + kCellWarpOut - 1) / kCellWarpOut;
     const int wpc = kCellThreads / 32;
     return dim3(a.nlines, (nwin + wpc - 1) / wpc);
 }
@@ -84,8 +85,9 @@ courant_kernel(const double* __restrict__ u, int nx, int ny, int nxt, long long 
         cx = omax(cx, cn);
         cy = omax(cy, ct);
     }
-    warp_max_atomic(&cour[0], cx);
-    warp_max_atomic(&cour[1], cy);
+    const int slot = cour_slot();
+    warp_max_atomic(&cour[slot], cx);
+    warp_max_atomic(&cour[kCourSlots + slot], cy);
 }
 
 int sweep_blocks_per_sm(int dir, bool unit_slope) {
@@ -166,13 +168,18 @@ __global__ void clock_begin_kernel(DevClock* c, unsigned long long* cour, double
         return;
     }
     if ((c->nstep % 2) == 0) {
-        const double cx = __longlong_as_double((long long)cour[0]);
-        const double cy = __longlong_as_double((long long)cour[1]);
+        unsigned long long mx = 0ull, my = 0ull;
+        for (int s = 0; s < kCourSlots; s++) {
+            mx = cour[s] > mx ? cour[s] : mx;
+            my = cour[kCourSlots + s] > my ? cour[kCourSlots + s] : my;
+            cour[s] = 0ull;
+            cour[kCourSlots + s] = 0ull;
+        }
+        const double cx = __longlong_as_double((long long)mx);
+        const double cy = __longlong_as_double((long long)my);
         double dt = courant_factor * dx / omax(cx, omax(cy, smallc));
         if (c->nstep == 0) dt = dt / 2.0;
         c->dt = dt;
-        cour[0] = 0ull;
-        cour[1] = 0ull;
     }
 }
 
@@ -231,13 +238,18 @@ __global__ void batch_clock_begin_kernel(BatchInst* inst, int nslots, double cou
         return;
     }
     if ((I.nstep % 2) == 0) {
-        const double cx = __longlong_as_double((long long)I.cour[0]);
-        const double cy = __longlong_as_double((long long)I.cour[1]);
+        unsigned long long mx = 0ull, my = 0ull;
+        for (int k = 0; k < kBatchCourSlots; k++) {
+            mx = I.cour[k] > mx ? I.cour[k] : mx;
+            my = I.cour[kBatchCourSlots + k] > my ? I.cour[kBatchCourSlots + k] : my;
+            I.cour[k] = 0ull;
+            I.cour[kBatchCourSlots + k] = 0ull;
+        }
+        const double cx = __longlong_as_double((long long)mx);
+        const double cy = __longlong_as_double((long long)my);
         double dt = courant_factor * I.dx / omax(cx, omax(cy, smallc));
         if (I.nstep == 0) dt = dt / 2.0;
         I.dt = dt;
-        I.cour[0] = 0ull;
-        I.cour[1] = 0ull;
     }
 }
 
@@ -283,8 +295,9 @@ batch_courant_kernel(BatchInst* inst, const int* slots, int nslots, Phys P) {
         cx = omax(cx, cn);
         cy = omax(cy, ct);
     }
-    warp_max_atomic(&Ip->cour[0], cx);
-    warp_max_atomic(&Ip->cour[1], cy);
+    const int slot = blockIdx.x % kBatchCourSlots;
+    warp_max_atomic(&Ip->cour[slot], cx);
+    warp_max_atomic(&Ip->cour[kBatchCourSlots + slot], cy);
 }
 
 // A single-blast initial state written on the device: density rho, zero

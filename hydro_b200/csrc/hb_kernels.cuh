@@ -28,7 +28,7 @@ struct SweepArgs {
     double* gout;            // ghost cells of the swept direction are written here (or null)
     const DevClock* clk;     // null: use dt below; else dt and the active flag come from here
     double dt;
-    unsigned long long* courant;  // null or [2]: fused max(c+|u|), max(c+|v|) (bit patterns)
+    unsigned long long* courant;  // null or [2 * kCourSlots] fused maxima (bit patterns)
     int nx, ny, nxt, nyt;
     long long vs;            // nxt * nyt (stride between variables)
     int bnd_lo, bnd_hi;      // boundary types of the swept direction (left/right or down/up)
@@ -38,6 +38,13 @@ struct SweepArgs {
 };
 
 constexpr int kSweepThreads = 64;
+
+// The fused Courant maxima are accumulated with atomicMax into kCourSlots
+// slots per direction ([0, kCourSlots): max(c+|u|), [kCourSlots, 2*kCourSlots):
+// max(c+|v|)), the slot chosen by the CTA index, so that no single address
+// takes one atomic per warp of the whole grid; readers take the max over the
+// slots (max is exact, so the result does not depend on the split).
+constexpr int kCourSlots = 128;
 
 // Launchers (hb_kernels.cu).  Each returns the cudaError_t of the launch.
 cudaError_t launch_sweep(int dir, const SweepArgs& a, const Phys& P, cudaStream_t s);

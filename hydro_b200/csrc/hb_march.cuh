@@ -100,6 +100,11 @@ __device__ __forceinline__ void store_cell(const SweepArgs& a, const LineGeom<DI
     p[3 * a.vs] = o.e;
 }
 
+// Slot of this CTA in a Courant accumulator array (see kCourSlots).
+__device__ __forceinline__ int cour_slot() {
+    return (int)((blockIdx.x + (unsigned long long)blockIdx.y * gridDim.x) % kCourSlots);
+}
+
 __device__ __forceinline__ void warp_max_atomic(unsigned long long* dst, double v) {
     for (int o = 16; o > 0; o >>= 1) {
         const double w = __shfl_xor_sync(0xffffffffu, v, o);
@@ -172,12 +177,25 @@ __device__ __forceinline__ void march(const SweepArgs& a, const typename S::Cons
     Prim xm2 = S::zero_prim();                      // qxm of k-2
     Flux fprev = S::zero_flux();                    // flux at (k-3 | k-2)
 
+    // y sweep of a stage set with S::prefetch: the next cell is loaded one
+    // iteration ahead, so its latency hides behind this iteration's
+    // arithmetic (costs registers; the FP64 set, bound by arithmetic, keeps
+    // its occupancy instead).
+    constexpr bool pre = DIR == 2 && S::prefetch;
+    Cons next = pre ? load_cell<DIR>(a, g, k0 - 2) : Cons{0.0, 0.0, 0.0, 0.0};
     for (int k = k0 - 2; k <= k1 + 1; k++) {
         Cons uk;
+        Cons u2{0.0, 0.0, 0.0, 0.0};
         if (DIR == 1) {
             if (((k - (k0 - 2)) & 3) == 0) ring.fill(a, reinterpret_cast<const LineGeom<1>&>(g), k,
                                                      k1 + 1, vec_ok);
             uk = (k >= 2 && k < a.n - 2) ? ring.cell(k) : load_cell<DIR>(a, g, k);
+        } else if (pre) {
+            uk = next;
+            if (k <= k1) next = load_cell<DIR>(a, g, k + 1);
+            // Cell k-2, updated in this iteration, is read again (a cache hit)
+            // instead of being carried in registers.
+            if (k >= k0 + 2) u2 = load_interior<DIR>(a, g, k - 2);
         } else {
             uk = load_cell<DIR>(a, g, k);
         }
@@ -194,9 +212,8 @@ __device__ __forceinline__ void march(const SweepArgs& a, const typename S::Cons
             if (k >= k0 + 1) {
                 f = S::riemann(C, xm2, xp1);
                 if (k >= k0 + 2) {
-                    // Cell k-2 is interior: its conservative values are read
-                    // again (the row ring, or a cache hit) instead of being carried.
-                    const Cons u2 = DIR == 1 ? ring.cell(k - 2) : load_interior<DIR>(a, g, k - 2);
+                    if (DIR == 1) u2 = ring.cell(k - 2);
+                    else if (!pre) u2 = load_interior<DIR>(a, g, k - 2);
                     const Cons o = S::update(u2, fprev, f, dtdx);
                     store_cell<DIR>(a, g, k - 2, o);
                     if (a.courant) {
@@ -242,8 +259,9 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, const Phys& P) {
         march<DIR, S>(a, C, g, k0, k1, dtdx, cx, cy);
     }
     if (a.courant) {
-        warp_max_atomic(&a.courant[0], cx);
-        warp_max_atomic(&a.courant[1], cy);
+        const int slot = cour_slot();
+        warp_max_atomic(&a.courant[slot], cx);
+        warp_max_atomic(&a.courant[kCourSlots + slot], cy);
     }
 }
 
@@ -275,7 +293,10 @@ __device__ __forceinline__ F flux_up(const F& f) {
 }
 
 
-// One warp's window: row `row`, output cells [c, c + 28) with c = 2 + 28 * win.
+// One warp's window: row `row`, output cells [c, c + 28) n [2, n - 2) with
+// c = 28 * win, computed from cells [c - 2, c + 30) (one per lane).  Windows
+// start at multiples of 28 cells (7 sectors of 4 doubles), so when the row
+// pitch is a multiple of 4 cells no 32-byte sector is written by two warps.
 // Accumulates the fused Courant maxima of its outputs into cx, cy.  The
 // caller guarantees the warp is converged and `row` < a.nlines.
 template <class S>
@@ -286,12 +307,12 @@ __device__ __forceinline__ void xcell_window(const SweepArgs& a, const typename 
     using Flux = typename S::Flux;
     using Real = typename S::Real;
     const int lane = threadIdx.x & 31;
-    const int c = 2 + win * kCellWarpOut;            // first output cell of the warp
+    const int c = win * kCellWarpOut;                // first output cell of the warp
     if (c >= a.n - 2) return;                        // warp-uniform
     const int k = c - 2 + lane;                      // this lane's cell
     const LineGeom<1> g(a, row);
     const typename S::TraceK K = S::trace_constants(C, dtdx);
-    const bool inside = k < a.n;                     // lanes past the row end idle
+    const bool inside = k >= 0 && k < a.n;           // lanes outside the row idle
     const Cons u = inside ? load_cell<1>(a, g, k) : Cons{1.0, 0.0, 0.0, 1.0};
     Prim q;
     Real cs;
@@ -304,7 +325,7 @@ __device__ __forceinline__ void xcell_window(const SweepArgs& a, const typename 
     const Prim xp_next = prim_down(xp);              // qxp of cell k + 1
     const Flux f = S::riemann(C, xm, xp_next);       // interface (k | k + 1)
     const Flux f_prev = flux_up(f);                  // interface (k - 1 | k)
-    if (lane >= 2 && lane < 2 + kCellWarpOut && k < a.n - 2) {
+    if (lane >= 2 && lane < 2 + kCellWarpOut && k >= 2 && k < a.n - 2) {
         const Cons o = S::update(u, f_prev, f, dtdx);
         store_cell<1>(a, g, k, o);
         if (a.courant) {
@@ -333,8 +354,9 @@ __device__ __forceinline__ void xcell_body(const SweepArgs& a, const Phys& P) {
         xcell_window<S>(a, C, row, win, dt / P.dx, cx, cy);
     }
     if (a.courant) {
-        warp_max_atomic(&a.courant[0], cx);
-        warp_max_atomic(&a.courant[1], cy);
+        const int slot = cour_slot();
+        warp_max_atomic(&a.courant[slot], cx);
+        warp_max_atomic(&a.courant[kCourSlots + slot], cy);
     }
 }
 

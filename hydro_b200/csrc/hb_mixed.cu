@@ -20,7 +20,7 @@ xcell_mixed_kernel(const SweepArgs a, const Phys P) {
 }
 
 cudaError_t launch_xcell_mixed(const SweepArgs& a, const Phys& P, cudaStream_t s) {
-    const int nwin = (a.n - 4 + kCellWarpOut - 1) / kCellWarpOut;
+    const int nwin = (a.n - 2 + kCellWarpOut - 1) / kCellWarpOut;
     const int wpc = kCellThreads / 32;
     dim3 grid(a.nlines, (nwin + wpc - 1) / wpc);
     xcell_mixed_kernel<<<grid, kCellThreads, 0, s>>>(a, P);

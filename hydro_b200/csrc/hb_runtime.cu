@@ -26,6 +26,8 @@ using hb::DevClock;
 using hb::Phys;
 using hb::SweepArgs;
 
+static constexpr size_t kCourBytes = 2 * hb::kCourSlots * sizeof(unsigned long long);
+
 // ---------------------------------------------------------------- errors
 static thread_local int g_err = HB_OK;
 static thread_local char g_msg[512] = "";
@@ -74,7 +76,7 @@ struct hb_domain {
     size_t nelem = 0;                  // 4 * nxt * nyt
     double* A = nullptr;               // resident state
     double* B = nullptr;               // scratch: output of the first sweep of a step
-    unsigned long long* cour = nullptr;  // [2] Courant maxima (bit patterns)
+    unsigned long long* cour = nullptr;  // [2 * kCourSlots] Courant maxima (bit patterns)
     DevClock* clk = nullptr;
     double* dts = nullptr;
     int ndts = 0;
@@ -203,9 +205,9 @@ static int domain_alloc(hb_domain* d) {
     HB_CU(cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking));
     HB_CU(cudaMalloc(&d->A, d->nelem * sizeof(double)));
     HB_CU(cudaMalloc(&d->B, d->nelem * sizeof(double)));
-    HB_CU(cudaMalloc(&d->cour, 2 * sizeof(unsigned long long)));
+    HB_CU(cudaMalloc(&d->cour, kCourBytes));
     HB_CU(cudaMalloc(&d->clk, sizeof(DevClock)));
-    HB_CU(cudaMemsetAsync(d->cour, 0, 2 * sizeof(unsigned long long), d->stream));
+    HB_CU(cudaMemsetAsync(d->cour, 0, kCourBytes, d->stream));
     HB_CU(cudaMemsetAsync(d->clk, 0, sizeof(DevClock), d->stream));
     return HB_OK;
 }
@@ -326,7 +328,7 @@ static int domain_step(hb_domain* d, int idim, double dt, const DevClock* clk, b
     const int first = (idim == 1) ? 1 : 2;
     const int second = 3 - first;
     if (fuse) {
-        HB_CU(cudaMemsetAsync(d->cour, 0, 2 * sizeof(unsigned long long), d->stream));
+        HB_CU(cudaMemsetAsync(d->cour, 0, kCourBytes, d->stream));
     }
     SweepArgs a1 = sweep_args(d, first, d->A, d->B, clk, dt, nullptr);
     int rc = launch_sweep_timed(d, first, a1);
@@ -411,7 +413,7 @@ extern "C" int hydro_b200_domain_make_boundary(hb_domain* d, int idim) {
 
 static int ensure_courant(hb_domain* d) {
     if (d->cour_valid) return HB_OK;
-    HB_CU(cudaMemsetAsync(d->cour, 0, 2 * sizeof(unsigned long long), d->stream));
+    HB_CU(cudaMemsetAsync(d->cour, 0, kCourBytes, d->stream));
     HB_CU(hb::launch_courant(d->A, d->nx, d->ny, d->nxt, d->vs, d->P, d->cour, d->stream));
     d->launches += 1;
     d->cour_valid = true;
@@ -422,12 +424,17 @@ extern "C" int hydro_b200_domain_courant(hb_domain* d, double* cx, double* cy) {
     if (!d) return set_error(HB_ERR_ARG, "null domain");
     int rc = ensure_courant(d);
     if (rc) return rc;
-    unsigned long long h[2];
+    unsigned long long h[2 * hb::kCourSlots];
     HB_CU(cudaMemcpyAsync(h, d->cour, sizeof(h), cudaMemcpyDeviceToHost, d->stream));
     HB_CU(cudaStreamSynchronize(d->stream));
+    unsigned long long mx = 0, my = 0;
+    for (int s = 0; s < hb::kCourSlots; s++) {
+        mx = h[s] > mx ? h[s] : mx;
+        my = h[hb::kCourSlots + s] > my ? h[hb::kCourSlots + s] : my;
+    }
     double x, y;
-    memcpy(&x, &h[0], 8);
-    memcpy(&y, &h[1], 8);
+    memcpy(&x, &mx, 8);
+    memcpy(&y, &my, 8);
     if (cx) *cx = x;
     if (cy) *cy = y;
     return HB_OK;

@@ -283,6 +283,7 @@ struct ExactStages {
     using Flux = Cons;
     using Real = double;
     using TraceK = hb::TraceK;
+    static constexpr bool prefetch = false;
     static __device__ __forceinline__ Consts consts(const Phys& P) { return P; }
     static __device__ __forceinline__ Prim zero_prim() { return Prim{0.0, 0.0, 0.0, 0.0}; }
     static __device__ __forceinline__ Flux zero_flux() { return Flux{0.0, 0.0, 0.0, 0.0}; }

@@ -36,13 +36,14 @@ struct TraceKF {
     float dtdx, zerol, zeror, project;
 };
 
-// Reciprocal and reciprocal square root in FP64 by Newton-Raphson from the
-// FP32 hardware approximation (about 23 correct bits; each step doubles them,
-// two steps reach the FP64 rounding level).  Valid for |x| in the normal
-// FP32 range, which every positive quantity of a valid state is in (the
-// smallest pressure is rho * smallc^2 / gamma >= ~1e-31).
+// Reciprocal and reciprocal square root in FP64: the hardware approximation
+// (PTX rcp.approx.ftz.f64 / rsqrt.approx.ftz.f64) refined by two
+// Newton-Raphson steps, each of which doubles the number of correct bits, to
+// the FP64 rounding level.  Inputs are positive normal numbers (every
+// divisor and radicand of a valid state is).
 __device__ __forceinline__ double rcp64(double x) {
-    double y = (double)(1.0f / (float)x);
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
     double e = fma(-x, y, 1.0);
     y = fma(y, e, y);
     e = fma(-x, y, 1.0);
@@ -50,7 +51,8 @@ __device__ __forceinline__ double rcp64(double x) {
 }
 
 __device__ __forceinline__ double rsqrt64(double x) {
-    double y = (double)rsqrtf((float)x);
+    double y;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
     double h = 0.5 * y;
     double r = fma(-(x * y), h, 0.5);  // 1/2 - x y^2 / 2
     y = fma(y, r, y);
@@ -62,9 +64,10 @@ __device__ __forceinline__ double rsqrt64(double x) {
 struct MixedStages {
     using Consts = MixedConsts;
     using Prim = PrimF;
-    using Flux = FluxF;
+    using Flux = Cons;   // the FP32 flux converted once to FP64 (exact)
     using Real = float;
     using TraceK = TraceKF;
+    static constexpr bool prefetch = true;
 
     static __device__ __forceinline__ Consts consts(const Phys& P) {
         Consts C;
@@ -88,7 +91,7 @@ struct MixedStages {
         return C;
     }
     static __device__ __forceinline__ Prim zero_prim() { return Prim{0.f, 0.f, 0.f, 0.f}; }
-    static __device__ __forceinline__ Flux zero_flux() { return Flux{0.f, 0.f, 0.f, 0.f}; }
+    static __device__ __forceinline__ Flux zero_flux() { return Flux{0.0, 0.0, 0.0, 0.0}; }
     static __device__ __forceinline__ bool second_order(const Consts& C) { return C.iorder != 1; }
 
     static __device__ __forceinline__ TraceK trace_constants(const Consts& C, double dtdx) {
@@ -237,17 +240,16 @@ struct MixedStages {
         const float mass = gr * gu;
         const float ekin = 0.5f * gr * (gu * gu + gv * gv);
         const float etot = gp * C.entho + ekin;
-        return Flux{mass, mass * gu + gp, mass * gv, gu * (etot + gp)};
+        const FluxF f{mass, mass * gu + gp, mass * gv, gu * (etot + gp)};
+        return Flux{(double)f.d, (double)f.mn, (double)f.mt, (double)f.e};
     }
 
     // FP64 update with the flux difference formed in FP64 (the FP32 fluxes
     // are exact in FP64, so no digits are lost to cancellation).
     static __device__ __forceinline__ Cons update(const Cons& u, const Flux& fl, const Flux& fr,
                                                   double dtdx) {
-        return Cons{fma((double)fl.d - (double)fr.d, dtdx, u.d),
-                    fma((double)fl.mn - (double)fr.mn, dtdx, u.mn),
-                    fma((double)fl.mt - (double)fr.mt, dtdx, u.mt),
-                    fma((double)fl.e - (double)fr.e, dtdx, u.e)};
+        return Cons{fma(fl.d - fr.d, dtdx, u.d), fma(fl.mn - fr.mn, dtdx, u.mn),
+                    fma(fl.mt - fr.mt, dtdx, u.mt), fma(fl.e - fr.e, dtdx, u.e)};
     }
 
     // Courant speeds of the updated cell in FP64 (ComputeQEforRow +
