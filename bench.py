@@ -166,6 +166,12 @@ def barrier(pg, device):
         pg.all_reduce(torch.zeros(1, device=device))
 
 
+def aggregate_mcs(world, cells_per_rank, steps, ms_max):
+    """Whole-job Mcell-updates/s of `world` replicas that each advanced
+    cells_per_rank cells by `steps` steps, timed as the slowest rank."""
+    return world * cells_per_rank * steps / (ms_max / 1e3) / 1e6
+
+
 def dom_state_after(H, u0, nsteps, precision):
     from hydro_b200 import Domain
     d = Domain(H, precision=precision)
@@ -364,7 +370,7 @@ def main():
     ms_max = all_max(pg, ms, device)
     t_end, n_end, dt_end = dom.get_clock()
     assert n_end == K, (n_end, K)
-    value = world * nx * ny * K / (ms_max / 1e3) / 1e6
+    value = aggregate_mcs(world, nx * ny, K, ms_max)
 
     # Per-launch duration of the sweep kernel: the same K steps again with an
     # event pair around every sweep launch.
