@@ -135,6 +135,8 @@ SIGNATURES = [
     ("hydro_b200_batch_bytes_needed", C.c_longlong, [_P]),
     ("hydro_b200_batch_arena_free", C.c_longlong, [_D]),
     ("hydro_b200_batch_add", C.c_int, [_D, _P, C.c_void_p, C.c_double, C.c_int]),
+    ("hydro_b200_batch_add_resume", C.c_int, [_D, _P, C.c_void_p, C.c_double, C.c_double,
+                                              C.c_int]),
     ("hydro_b200_batch_add_blast", C.c_int, [_D, _P, C.c_double, C.c_double, C.c_int, C.c_int,
                                              C.c_double, C.c_double, C.c_int]),
     ("hydro_b200_batch_remove", C.c_int, [_D, C.c_int]),

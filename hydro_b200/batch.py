@@ -29,6 +29,7 @@ class Batch:
             raise _lib.HydroB200Error("batch creation failed")
         self.capacity = capacity
         self.params = {}
+        self.limits = {}
 
     @staticmethod
     def bytes_needed(H: HydroParam) -> int:
@@ -65,6 +66,7 @@ class Batch:
                 raise _lib.HydroB200Error(f"batch add failed ({err}): {msg}")
             return -1
         self.params[slot] = H
+        self.limits[slot] = (tend, nstepmax)
         return slot
 
     def try_add_blast(self, H: HydroParam, rho: float, e_bg: float, cell: tuple, e_blast: float,
@@ -81,11 +83,44 @@ class Batch:
                 raise _lib.HydroB200Error(f"batch add failed ({err}): {msg}")
             return -1
         self.params[slot] = H
+        self.limits[slot] = (tend, nstepmax)
+        return slot
+
+    def checkpoint(self, slot: int) -> dict:
+        """State and clock of an instance (with its grid parameters and
+        limits), enough to resume it bit for bit later, here or in another
+        batch."""
+        st = self.status(slot)
+        H = self.params[slot]
+        return {"state": self.download(slot), "t": st["t"], "nstep": st["nstep"],
+                "dt": st["dt"], "nx": H.nx, "ny": H.ny, "dx": H.dx,
+                "boundary": (H.boundary_left, H.boundary_right, H.boundary_down,
+                             H.boundary_up),
+                "tend": self.limits.get(slot, (1e300, 2**31 - 1))[0],
+                "nstepmax": self.limits.get(slot, (1e300, 2**31 - 1))[1]}
+
+    def resume(self, ckpt: dict) -> int:
+        """Admit a checkpointed instance; returns its slot (-1 when full)."""
+        H = make_params(ckpt["nx"], ckpt["ny"], dx=ckpt["dx"], boundary=tuple(ckpt["boundary"]))
+        H.t = ckpt["t"]
+        H.nstep = ckpt["nstep"]
+        state = np.ascontiguousarray(ckpt["state"], dtype=np.float64)
+        slot = self.lib.hydro_b200_batch_add_resume(self.h, C.byref(H), state.ctypes.data,
+                                                    ckpt["dt"], ckpt["tend"], ckpt["nstepmax"])
+        if slot < 0:
+            err = self.lib.hydro_b200_last_error()
+            self.lib.hydro_b200_clear_error()
+            if err != _lib.HB_ERR_NOMEM:
+                raise _lib.HydroB200Error(f"batch resume failed ({err})")
+            return -1
+        self.params[slot] = H
+        self.limits[slot] = (ckpt["tend"], ckpt["nstepmax"])
         return slot
 
     def remove(self, slot: int) -> None:
         check(self.lib.hydro_b200_batch_remove(self.h, slot))
         self.params.pop(slot, None)
+        self.limits.pop(slot, None)
 
     def steps(self, n: int) -> None:
         check(self.lib.hydro_b200_batch_steps(self.h, n))

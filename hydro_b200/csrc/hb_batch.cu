@@ -114,13 +114,14 @@ struct hb_batch {
     // arena
     Arena arena;
     double* arena_mem = nullptr;
-    // work lists (two: the first and second sweeps of an even-parity step)
-    WorkItem* items_d[2] = {nullptr, nullptr};
-    int nitems[2] = {0, 0};
-    int items_cap[2] = {0, 0};
+    // work lists: [list][dir-1]; list 0 holds the first sweeps of an
+    // even-parity step, list 1 the second sweeps; one list per direction
+    WorkItem* items_d[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    int nitems[2][2] = {{0, 0}, {0, 0}};
+    int items_cap[2][2] = {{0, 0}, {0, 0}};
     long long lists_step = -1;       // global step the lists' parities refer to
     bool lists_dirty = true;
-    unsigned int* counters = nullptr;  // [2]
+    unsigned int* counters = nullptr;  // [2 phases][2 directions]
     // graphs for the two step parities
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     bool graphs_dirty = true;
@@ -152,49 +153,44 @@ int sync_table_up(hb_batch* b) {
     return HB_OK;
 }
 
-int ensure_items(hb_batch* b, int which, int n) {
-    if (n <= b->items_cap[which]) return HB_OK;
-    cudaFree(b->items_d[which]);
-    b->items_d[which] = nullptr;
-    b->items_cap[which] = 0;
-    HB_BCU(cudaMalloc(&b->items_d[which], sizeof(WorkItem) * (size_t)std::max(n, 1)));
-    b->items_cap[which] = n;
+int ensure_items(hb_batch* b, int list, int d, int n) {
+    if (n <= b->items_cap[list][d]) return HB_OK;
+    cudaFree(b->items_d[list][d]);
+    b->items_d[list][d] = nullptr;
+    b->items_cap[list][d] = 0;
+    HB_BCU(cudaMalloc(&b->items_d[list][d], sizeof(WorkItem) * (size_t)std::max(n, 1)));
+    b->items_cap[list][d] = n;
     return HB_OK;
 }
 
 // Lists for the current global step: list 0 holds each active instance's
 // first-sweep items (x on even nstep, y on odd), list 1 its second-sweep
-// items.  Big (y) items first so the queue's tail is made of small ones.
+// items, each split by direction.
 int build_lists(hb_batch* b) {
-    std::vector<WorkItem> L[2];
-    for (int pass = 0; pass < 2; pass++) {
-        for (int s = 0; s < b->capacity; s++) {
-            const BatchInst& I = b->h[s];
-            if (b->off[s] < 0 || !I.active) continue;
-            const bool even = (I.nstep % 2) == 0;
-            // pass 0: y items, pass 1: x items.
-            const int dir = pass == 0 ? 2 : 1;
-            const int list = (dir == 1) == even ? 0 : 1;
-            if (dir == 2) {
-                for (int l0 = 0; l0 < I.nx; l0 += hb::kBatchThreads)
-                    for (int k0 = 2; k0 < I.ny + 2; k0 += b->tune.seg)
-                        L[list].push_back(WorkItem{s, 2, l0, k0});
-            } else {
-                const int nwin = (I.nx + 2 + hb::kCellWarpOut - 1) / hb::kCellWarpOut;
-                for (int l = 0; l < I.ny; l++)
-                    for (int w0 = 0; w0 < nwin; w0 += hb::kXItemWindows)
-                        L[list].push_back(WorkItem{s, 1, l, w0});
-            }
+    std::vector<WorkItem> L[2][2];
+    for (int s = 0; s < b->capacity; s++) {
+        const BatchInst& I = b->h[s];
+        if (b->off[s] < 0 || !I.active) continue;
+        const bool even = (I.nstep % 2) == 0;
+        const int xl = even ? 0 : 1, yl = 1 - xl;
+        for (int l0 = 0; l0 < I.nx; l0 += hb::kBatchThreads)
+            for (int k0 = 2; k0 < I.ny + 2; k0 += b->tune.seg)
+                L[yl][1].push_back(WorkItem{s, 2, l0, k0});
+        const int nwin = (I.nx + 2 + hb::kCellWarpOut - 1) / hb::kCellWarpOut;
+        for (int l = 0; l < I.ny; l++)
+            for (int w0 = 0; w0 < nwin; w0 += hb::kXItemWindows)
+                L[xl][0].push_back(WorkItem{s, 1, l, w0});
+    }
+    for (int w = 0; w < 2; w++)
+        for (int d = 0; d < 2; d++) {
+            int rc = ensure_items(b, w, d, (int)L[w][d].size());
+            if (rc) return rc;
+            if (!L[w][d].empty())
+                HB_BCU(cudaMemcpyAsync(b->items_d[w][d], L[w][d].data(),
+                                       sizeof(WorkItem) * L[w][d].size(), cudaMemcpyHostToDevice,
+                                       b->stream));
+            b->nitems[w][d] = (int)L[w][d].size();
         }
-    }
-    for (int w = 0; w < 2; w++) {
-        int rc = ensure_items(b, w, (int)L[w].size());
-        if (rc) return rc;
-        if (!L[w].empty())
-            HB_BCU(cudaMemcpyAsync(b->items_d[w], L[w].data(), sizeof(WorkItem) * L[w].size(),
-                                   cudaMemcpyHostToDevice, b->stream));
-        b->nitems[w] = (int)L[w].size();
-    }
     HB_BCU(cudaStreamSynchronize(b->stream));
     b->lists_step = b->gstep;
     b->lists_dirty = false;
@@ -202,9 +198,9 @@ int build_lists(hb_batch* b) {
     return HB_OK;
 }
 
-int grid_size(hb_batch* b) {
+int grid_size(hb_batch* b, int dir) {
     const int occ = hb::batch_sweep_blocks_per_sm(b->precision == HB_PREC_MIXED,
-                                                  b->P.unit_slope != 0);
+                                                  b->P.unit_slope != 0, dir);
     const int per = (b->tune.blocks_per_sm > 0 && b->tune.blocks_per_sm < occ)
                         ? b->tune.blocks_per_sm
                         : occ;
@@ -212,18 +208,21 @@ int grid_size(hb_batch* b) {
 }
 
 int launch_sweep(hb_batch* b, int list, int phase, cudaStream_t s) {
-    BatchLaunch L;
-    L.inst = b->d;
-    L.items = b->items_d[list];
-    L.nitems = b->nitems[list];
-    L.phase = phase;
-    L.counter = b->counters + (phase - 1);
-    L.seg = b->tune.seg;
-    L.claim = b->tune.claim;
-    if (L.nitems == 0) return HB_OK;
-    const int grid = grid_size(b);
-    HB_BCU(b->precision == HB_PREC_MIXED ? hb::launch_batch_sweep_mixed(L, b->P, grid, s)
-                                         : hb::launch_batch_sweep(L, b->P, grid, s));
+    for (int dir = 1; dir <= 2; dir++) {
+        BatchLaunch L;
+        L.inst = b->d;
+        L.items = b->items_d[list][dir - 1];
+        L.nitems = b->nitems[list][dir - 1];
+        L.phase = phase;
+        L.counter = b->counters + 2 * (phase - 1) + (dir - 1);
+        L.seg = b->tune.seg;
+        L.claim = b->tune.claim;
+        if (L.nitems == 0) continue;
+        const int grid = grid_size(b, dir);
+        HB_BCU(b->precision == HB_PREC_MIXED
+                   ? hb::launch_batch_sweep_mixed(L, b->P, dir, grid, s)
+                   : hb::launch_batch_sweep(L, b->P, dir, grid, s));
+    }
     return HB_OK;
 }
 
@@ -231,7 +230,7 @@ int launch_sweep(hb_batch* b, int list, int phase, cudaStream_t s) {
 int record_step(hb_batch* b, int flip, cudaStream_t s) {
     HB_BCU(hb::launch_batch_clock_begin(b->d, b->capacity, b->courant_factor, b->P.smallc,
                                         b->gstep_d, s));
-    HB_BCU(cudaMemsetAsync(b->counters, 0, 2 * sizeof(unsigned int), s));
+    HB_BCU(cudaMemsetAsync(b->counters, 0, 4 * sizeof(unsigned int), s));
     int rc = launch_sweep(b, flip, 1, s);
     if (rc) return rc;
     rc = launch_sweep(b, 1 - flip, 2, s);
@@ -267,7 +266,8 @@ int prepare(hb_batch* b) {
     if (!b->fresh.empty()) {
         HB_BCU(cudaMemcpyAsync(b->fresh_d, b->fresh.data(), sizeof(int) * b->fresh.size(),
                                cudaMemcpyHostToDevice, b->stream));
-        HB_BCU(hb::launch_batch_courant(b->d, b->fresh_d, (int)b->fresh.size(), b->P, b->stream));
+        HB_BCU(hb::launch_batch_courant(b->d, b->fresh_d, (int)b->fresh.size(), b->P,
+                                        b->precision == HB_PREC_MIXED, b->stream));
         b->launches += 1;
         b->fresh.clear();
     }
@@ -349,7 +349,7 @@ extern "C" hb_batch* hydro_b200_batch_create(const hydroparam_t* H, int capacity
     if ((e = cudaMalloc(&b->d, sizeof(BatchInst) * capacity)) != cudaSuccess)
         return bad(e, "slot table");
     if ((e = cudaMalloc(&b->gstep_d, sizeof(long long))) != cudaSuccess) return bad(e, "counter");
-    if ((e = cudaMalloc(&b->counters, 2 * sizeof(unsigned int))) != cudaSuccess)
+    if ((e = cudaMalloc(&b->counters, 4 * sizeof(unsigned int))) != cudaSuccess)
         return bad(e, "counters");
     if ((e = cudaMalloc(&b->fresh_d, sizeof(int) * capacity)) != cudaSuccess)
         return bad(e, "fresh list");
@@ -369,7 +369,8 @@ extern "C" void hydro_b200_batch_destroy(hb_batch* b) {
     if (b->stream) cudaStreamSynchronize(b->stream);
     for (int f = 0; f < 2; f++)
         if (b->graph[f]) cudaGraphExecDestroy(b->graph[f]);
-    for (int w = 0; w < 2; w++) cudaFree(b->items_d[w]);
+    for (int w = 0; w < 2; w++)
+        for (int d = 0; d < 2; d++) cudaFree(b->items_d[w][d]);
     cudaFree(b->d);
     cudaFree(b->gstep_d);
     cudaFree(b->counters);
@@ -392,8 +393,24 @@ extern "C" long long hydro_b200_batch_bytes_needed(const hydroparam_t* H) {
 // Admit an instance: its grid (nx, ny, dx, boundary types) from H, its state
 // from host memory (reference layout), clock from t = H->t, nstep = H->nstep.
 // Returns the slot, or -1 (no free slot or arena space: HB_ERR_NOMEM).
+static int batch_add_impl(hb_batch* b, const hydroparam_t* H, const double* host, double tend,
+                          int nstepmax, double dt0);
+
 extern "C" int hydro_b200_batch_add(hb_batch* b, const hydroparam_t* H, const double* host,
                                     double tend, int nstepmax) {
+    return batch_add_impl(b, H, host, tend, nstepmax, 0.0);
+}
+
+// Resume a checkpointed instance: state from host memory, clock from
+// (H->t, H->nstep) and the dt of its last even step (needed when nstep is
+// odd: main.c keeps dt for the odd step that follows an even one).
+extern "C" int hydro_b200_batch_add_resume(hb_batch* b, const hydroparam_t* H, const double* host,
+                                           double dt, double tend, int nstepmax) {
+    return batch_add_impl(b, H, host, tend, nstepmax, dt);
+}
+
+static int batch_add_impl(hb_batch* b, const hydroparam_t* H, const double* host, double tend,
+                          int nstepmax, double dt0) {
     if (!b || !H || !host) return fail(HB_ERR_ARG, "add: null argument"), -1;
     if (H->nx < 3 || H->ny < 3 || !(H->dx > 0.0) ||
         (long long)(H->nx + 4) * (H->ny + 4) > (1ll << 31))
@@ -424,7 +441,7 @@ extern "C" int hydro_b200_batch_add(hb_batch* b, const hydroparam_t* H, const do
     I.bnd_up = H->boundary_up;
     I.dx = H->dx;
     I.t = H->t;
-    I.dt = 0.0;
+    I.dt = dt0;
     I.tend = tend;
     I.nstep = H->nstep;
     I.nstepmax = nstepmax;
@@ -516,7 +533,7 @@ extern "C" int hydro_b200_batch_steps(hb_batch* b, int n) {
         const int flip = (int)((b->gstep - b->lists_step) & 1);
         HB_BCU(cudaGraphLaunch(b->graph[flip], b->stream));
         b->gstep++;
-        b->launches += 4;
+        b->launches += 6;
     }
     return HB_OK;
 }
@@ -619,7 +636,7 @@ extern "C" int hydro_b200_batch_autotune(hb_batch* b, int steps) {
     static const int segs[] = {32, 64, 128};
     static const int claims[] = {1, 4, 16};
     const int occ = hb::batch_sweep_blocks_per_sm(b->precision == HB_PREC_MIXED,
-                                                  b->P.unit_slope != 0);
+                                                  b->P.unit_slope != 0, 2);
     const int bpsms[] = {0, std::max(1, occ / 2)};
     cudaEvent_t e0, e1;
     if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)

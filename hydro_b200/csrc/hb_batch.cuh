@@ -46,6 +46,9 @@ struct WorkItem {
 
 constexpr int kBatchThreads = 64;   // CTA of the batched sweep (two warps)
 constexpr int kBatchCourSlots = 16; // Courant accumulator slots per instance
+// Resident CTAs per SM the x-item kernels are compiled for (a register cap
+// that keeps the cell-per-lane work near the occupancy of the plain x sweep).
+constexpr int kBatchXMinBlocks = 10;
 constexpr int kXItemWindows = 8;    // cell windows per x item (4 per warp)
 
 struct BatchLaunch {
@@ -59,18 +62,23 @@ struct BatchLaunch {
 };
 
 // Launchers (hb_kernels.cu for FP64, hb_mixed.cu for the mixed form).
-cudaError_t launch_batch_sweep(const BatchLaunch& L, const Phys& P, int grid, cudaStream_t s);
-cudaError_t launch_batch_sweep_mixed(const BatchLaunch& L, const Phys& P, int grid,
+// One launch sweeps the items of one direction (dir 1: x, 2: y).
+cudaError_t launch_batch_sweep(const BatchLaunch& L, const Phys& P, int dir, int grid,
+                               cudaStream_t s);
+cudaError_t launch_batch_sweep_mixed(const BatchLaunch& L, const Phys& P, int dir, int grid,
                                      cudaStream_t s);
-int batch_sweep_blocks_per_sm(bool mixed, bool unit_slope);
+int batch_sweep_blocks_per_sm(bool mixed, bool unit_slope, int dir);
 cudaError_t launch_batch_clock_begin(BatchInst* inst, int nslots, double courant_factor,
                                      double smallc, long long* gstep, cudaStream_t s);
 cudaError_t launch_batch_clock_end(BatchInst* inst, int nslots, long long* gstep,
                                    cudaStream_t s);
 cudaError_t launch_blast_init(double* u, int nx, int ny, double rho, double ebg, int bi, int bj,
                               double eblast, cudaStream_t s);
-// Courant maxima of the listed instances' current states (slot per entry).
+// Courant maxima of the listed instances' current states (slot per entry),
+// with the per-cell formula of the batch's precision.
 cudaError_t launch_batch_courant(BatchInst* inst, const int* slots, int nslots, const Phys& P,
-                                 cudaStream_t s);
+                                 bool mixed, cudaStream_t s);
+cudaError_t launch_batch_courant_mixed(BatchInst* inst, const int* slots, int nslots,
+                                       const Phys& P, cudaStream_t s);
 
 }  // namespace hb

@@ -37,10 +37,13 @@ __device__ __forceinline__ SweepArgs batch_args(const BatchInst& I, int dir, int
     return a;
 }
 
-// Persistent CTAs claim `claim` items at a time until the list is exhausted.
-// An item's instance is skipped once its clock has stopped.  The second
-// sweep of an instance's odd step also reduces its Courant maxima.
-template <class S>
+// Persistent CTAs claim `claim` items at a time until the list is exhausted;
+// every item of the list sweeps direction DIR (x: cell-per-lane windows of a
+// row, y: marching 64-column groups), so each direction has its own kernel
+// with its own register budget.  An item's instance is skipped once its clock
+// has stopped.  The second sweep of an instance's odd step also reduces its
+// Courant maxima.
+template <class S, int DIR>
 __device__ __forceinline__ void batch_sweep_body(const BatchLaunch& L, const Phys& P) {
     __shared__ int s_base;
     const typename S::Consts C = S::consts(P);
@@ -57,10 +60,10 @@ __device__ __forceinline__ void batch_sweep_body(const BatchLaunch& L, const Phy
             const BatchInst I = *Ip;
             if (!I.active) continue;  // CTA-uniform
             const bool fuse = (L.phase == 2) && (I.nstep & 1);
-            const SweepArgs a = batch_args(I, w.dir, L.phase, fuse, Ip);
+            const SweepArgs a = batch_args(I, DIR, L.phase, fuse, Ip);
             const double dtdx = I.dt / I.dx;
             double cx = 0.0, cy = 0.0;
-            if (w.dir == 1) {
+            if (DIR == 1) {
                 const int warp = threadIdx.x >> 5;
                 for (int win = w.k0 + warp; win < w.k0 + kXItemWindows; win += kBatchThreads / 32)
                     xcell_window<S>(a, C, w.line, win, dtdx, cx, cy);
@@ -79,6 +82,18 @@ __device__ __forceinline__ void batch_sweep_body(const BatchLaunch& L, const Phy
             }
         }
     }
+}
+
+// The standalone Courant maxima of listed batch instances (grid y = entry).
+template <class S>
+__device__ __forceinline__ void batch_courant_body(BatchInst* inst, const int* slots, int nslots,
+                                                   const Phys& P) {
+    const int e = blockIdx.y;
+    if (e >= nslots) return;
+    BatchInst* Ip = inst + slots[e];
+    const int slot = blockIdx.x % kBatchCourSlots;
+    courant_body<S>(Ip->A, Ip->nx, Ip->ny, Ip->nxt, Ip->vs, P, &Ip->cour[slot],
+                    &Ip->cour[kBatchCourSlots + slot]);
 }
 
 }  // namespace hb

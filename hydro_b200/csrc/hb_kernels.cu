@@ -73,21 +73,8 @@ cudaError_t launch_sweep(int dir, const SweepArgs& a, const Phys& P, cudaStream_
 __global__ void __launch_bounds__(256)
 courant_kernel(const double* __restrict__ u, int nx, int ny, int nxt, long long vs, Phys P,
                unsigned long long* cour) {
-    double cx = 0.0, cy = 0.0;
-    const long long total = (long long)nx * ny;
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < total;
-         c += (long long)gridDim.x * blockDim.x) {
-        const int j = (int)(c / nx) + 2, i = (int)(c % nx) + 2;
-        const long long o = i + (long long)nxt * j;
-        Cons w{__ldg(u + o), __ldg(u + o + vs), __ldg(u + o + 2 * vs), __ldg(u + o + 3 * vs)};
-        double cn, ct;
-        courant_speeds(P, w, cn, ct);
-        cx = omax(cx, cn);
-        cy = omax(cy, ct);
-    }
     const int slot = cour_slot();
-    warp_max_atomic(&cour[slot], cx);
-    warp_max_atomic(&cour[kCourSlots + slot], cy);
+    courant_body<ExactStages<true>>(u, nx, ny, nxt, vs, P, &cour[slot], &cour[kCourSlots + slot]);
 }
 
 int sweep_blocks_per_sm(int dir, bool unit_slope) {
@@ -204,25 +191,36 @@ cudaError_t launch_clock_end(DevClock* c, cudaStream_t s) {
 }
 
 // ---------------------------------------------------------------- batches
-template <bool UNIT>
-__global__ void __launch_bounds__(kBatchThreads)
+template <bool UNIT, int DIR>
+__global__ void __launch_bounds__(kBatchThreads, DIR == 1 ? kBatchXMinBlocks : 1)
 batch_sweep_kernel(const BatchLaunch L, const Phys P) {
-    batch_sweep_body<ExactStages<UNIT>>(L, P);
+    batch_sweep_body<ExactStages<UNIT>, DIR>(L, P);
 }
 
-cudaError_t launch_batch_sweep(const BatchLaunch& L, const Phys& P, int grid, cudaStream_t s) {
-    if (P.unit_slope) batch_sweep_kernel<true><<<grid, kBatchThreads, 0, s>>>(L, P);
-    else batch_sweep_kernel<false><<<grid, kBatchThreads, 0, s>>>(L, P);
+cudaError_t launch_batch_sweep(const BatchLaunch& L, const Phys& P, int dir, int grid,
+                               cudaStream_t s) {
+    if (dir == 1) {
+        if (P.unit_slope) batch_sweep_kernel<true, 1><<<grid, kBatchThreads, 0, s>>>(L, P);
+        else batch_sweep_kernel<false, 1><<<grid, kBatchThreads, 0, s>>>(L, P);
+    } else {
+        if (P.unit_slope) batch_sweep_kernel<true, 2><<<grid, kBatchThreads, 0, s>>>(L, P);
+        else batch_sweep_kernel<false, 2><<<grid, kBatchThreads, 0, s>>>(L, P);
+    }
     return cudaGetLastError();
 }
 
-int batch_sweep_blocks_per_sm_exact(bool unit_slope) {
+template <class K>
+static int occupancy(K kernel) {
     int n = 0;
-    cudaError_t e = unit_slope ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                                     &n, batch_sweep_kernel<true>, kBatchThreads, 0)
-                               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                                     &n, batch_sweep_kernel<false>, kBatchThreads, 0);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, kBatchThreads, 0);
     return (e == cudaSuccess && n > 0) ? n : 1;
+}
+
+int batch_sweep_blocks_per_sm_exact(bool unit_slope, int dir) {
+    if (dir == 1) return unit_slope ? occupancy(batch_sweep_kernel<true, 1>)
+                                    : occupancy(batch_sweep_kernel<false, 1>);
+    return unit_slope ? occupancy(batch_sweep_kernel<true, 2>)
+                      : occupancy(batch_sweep_kernel<false, 2>);
 }
 
 // main.c:349-392 per instance (see clock_begin_kernel).
@@ -276,28 +274,10 @@ cudaError_t launch_batch_clock_end(BatchInst* inst, int nslots, long long* gstep
     return cudaGetLastError();
 }
 
-// Courant maxima of the listed instances (one CTA row-stride per instance).
+// Courant maxima of the listed instances (grid y: one instance per entry).
 __global__ void __launch_bounds__(256)
 batch_courant_kernel(BatchInst* inst, const int* slots, int nslots, Phys P) {
-    const int e = blockIdx.y;
-    if (e >= nslots) return;
-    BatchInst* Ip = inst + slots[e];
-    const BatchInst I = *Ip;
-    double cx = 0.0, cy = 0.0;
-    const long long total = (long long)I.nx * I.ny;
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < total;
-         c += (long long)gridDim.x * blockDim.x) {
-        const int j = (int)(c / I.nx) + 2, i = (int)(c % I.nx) + 2;
-        const double* u = I.A + i + (long long)I.nxt * j;
-        const Cons w{u[0], u[I.vs], u[2 * I.vs], u[3 * I.vs]};
-        double cn, ct;
-        courant_speeds(P, w, cn, ct);
-        cx = omax(cx, cn);
-        cy = omax(cy, ct);
-    }
-    const int slot = blockIdx.x % kBatchCourSlots;
-    warp_max_atomic(&Ip->cour[slot], cx);
-    warp_max_atomic(&Ip->cour[kBatchCourSlots + slot], cy);
+    batch_courant_body<ExactStages<true>>(inst, slots, nslots, P);
 }
 
 // A single-blast initial state written on the device: density rho, zero
@@ -328,8 +308,9 @@ cudaError_t launch_blast_init(double* u, int nx, int ny, double rho, double ebg,
 }
 
 cudaError_t launch_batch_courant(BatchInst* inst, const int* slots, int nslots, const Phys& P,
-                                 cudaStream_t s) {
+                                 bool mixed, cudaStream_t s) {
     if (nslots <= 0) return cudaSuccess;
+    if (mixed) return launch_batch_courant_mixed(inst, slots, nslots, P, s);
     batch_courant_kernel<<<dim3(16, nslots), 256, 0, s>>>(inst, slots, nslots, P);
     return cudaGetLastError();
 }

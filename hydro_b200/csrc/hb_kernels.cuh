@@ -60,6 +60,8 @@ cudaError_t launch_sweep_mixed(int dir, const SweepArgs& a, const Phys& P, cudaS
 int sweep_mixed_blocks_per_sm(int dir);
 cudaError_t launch_courant(const double* u, int nx, int ny, int nxt, long long vs, const Phys& P,
                            unsigned long long* cour, cudaStream_t s);
+cudaError_t launch_courant_mixed(const double* u, int nx, int ny, int nxt, long long vs,
+                                 const Phys& P, unsigned long long* cour, cudaStream_t s);
 cudaError_t launch_boundary(double* u, int idim, int nx, int ny, int nxt, int nyt, long long vs,
                             int bnd_lo, int bnd_hi, cudaStream_t s);
 cudaError_t launch_clock_begin(DevClock* c, unsigned long long* cour, double courant_factor,

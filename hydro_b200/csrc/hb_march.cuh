@@ -360,4 +360,29 @@ __device__ __forceinline__ void xcell_body(const SweepArgs& a, const Phys& P) {
     }
 }
 
+// The standalone Courant reduction (compute_deltat.c:54-73) over the interior
+// of one state, with the stage set's per-cell formula so that it agrees with
+// the reduction fused into the sweeps of the same precision.
+template <class S>
+__device__ __forceinline__ void courant_body(const double* __restrict__ u, int nx, int ny,
+                                             int nxt, long long vs, const Phys& P,
+                                             unsigned long long* cour_x,
+                                             unsigned long long* cour_y) {
+    const typename S::Consts C = S::consts(P);
+    double cx = 0.0, cy = 0.0;
+    const long long total = (long long)nx * ny;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < total;
+         c += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(c / nx) + 2, i = (int)(c % nx) + 2;
+        const long long o = i + (long long)nxt * j;
+        const Cons w{__ldg(u + o), __ldg(u + o + vs), __ldg(u + o + 2 * vs), __ldg(u + o + 3 * vs)};
+        double cn, ct;
+        S::courant(C, w, cn, ct);
+        cx = cx > cn ? cx : cn;
+        cy = cy > ct ? cy : ct;
+    }
+    warp_max_atomic(cour_x, cx);
+    warp_max_atomic(cour_y, cy);
+}
+
 }  // namespace hb

@@ -46,24 +46,56 @@ int sweep_mixed_blocks_per_sm(int dir) {
     return (e == cudaSuccess && n > 0) ? n : 1;
 }
 
-__global__ void __launch_bounds__(kBatchThreads)
+template <int DIR>
+__global__ void __launch_bounds__(kBatchThreads, DIR == 1 ? kBatchXMinBlocks : 1)
 batch_sweep_mixed_kernel(const BatchLaunch L, const Phys P) {
-    batch_sweep_body<MixedStages>(L, P);
+    batch_sweep_body<MixedStages, DIR>(L, P);
 }
 
-cudaError_t launch_batch_sweep_mixed(const BatchLaunch& L, const Phys& P, int grid,
+cudaError_t launch_batch_sweep_mixed(const BatchLaunch& L, const Phys& P, int dir, int grid,
                                      cudaStream_t s) {
-    batch_sweep_mixed_kernel<<<grid, kBatchThreads, 0, s>>>(L, P);
+    if (dir == 1) batch_sweep_mixed_kernel<1><<<grid, kBatchThreads, 0, s>>>(L, P);
+    else batch_sweep_mixed_kernel<2><<<grid, kBatchThreads, 0, s>>>(L, P);
     return cudaGetLastError();
 }
 
-int batch_sweep_blocks_per_sm_exact(bool unit_slope);  // hb_kernels.cu
+__global__ void __launch_bounds__(256)
+courant_mixed_kernel(const double* __restrict__ u, int nx, int ny, int nxt, long long vs, Phys P,
+                     unsigned long long* cour) {
+    const int slot = cour_slot();
+    courant_body<MixedStages>(u, nx, ny, nxt, vs, P, &cour[slot], &cour[kCourSlots + slot]);
+}
 
-int batch_sweep_blocks_per_sm(bool mixed, bool unit_slope) {
-    if (!mixed) return batch_sweep_blocks_per_sm_exact(unit_slope);
+cudaError_t launch_courant_mixed(const double* u, int nx, int ny, int nxt, long long vs,
+                                 const Phys& P, unsigned long long* cour, cudaStream_t s) {
+    const long long total = (long long)nx * ny;
+    long long blocks = (total + 255) / 256;
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    if (blocks < 1) blocks = 1;
+    courant_mixed_kernel<<<(unsigned)blocks, 256, 0, s>>>(u, nx, ny, nxt, vs, P, cour);
+    return cudaGetLastError();
+}
+
+__global__ void __launch_bounds__(256)
+batch_courant_mixed_kernel(BatchInst* inst, const int* slots, int nslots, Phys P) {
+    batch_courant_body<MixedStages>(inst, slots, nslots, P);
+}
+
+cudaError_t launch_batch_courant_mixed(BatchInst* inst, const int* slots, int nslots,
+                                       const Phys& P, cudaStream_t s) {
+    batch_courant_mixed_kernel<<<dim3(16, nslots), 256, 0, s>>>(inst, slots, nslots, P);
+    return cudaGetLastError();
+}
+
+int batch_sweep_blocks_per_sm_exact(bool unit_slope, int dir);  // hb_kernels.cu
+
+int batch_sweep_blocks_per_sm(bool mixed, bool unit_slope, int dir) {
+    if (!mixed) return batch_sweep_blocks_per_sm_exact(unit_slope, dir);
     int n = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_sweep_mixed_kernel,
-                                                                  kBatchThreads, 0);
+    cudaError_t e = dir == 1 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                                   &n, batch_sweep_mixed_kernel<1>, kBatchThreads, 0)
+                             : cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                                   &n, batch_sweep_mixed_kernel<2>, kBatchThreads, 0);
     return (e == cudaSuccess && n > 0) ? n : 1;
 }
 

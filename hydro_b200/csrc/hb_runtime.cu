@@ -414,7 +414,13 @@ extern "C" int hydro_b200_domain_make_boundary(hb_domain* d, int idim) {
 static int ensure_courant(hb_domain* d) {
     if (d->cour_valid) return HB_OK;
     HB_CU(cudaMemsetAsync(d->cour, 0, kCourBytes, d->stream));
-    HB_CU(hb::launch_courant(d->A, d->nx, d->ny, d->nxt, d->vs, d->P, d->cour, d->stream));
+    // The per-cell formula of the domain's precision, as in the fused reduction.
+    if (d->precision == HB_PREC_MIXED) {
+        HB_CU(hb::launch_courant_mixed(d->A, d->nx, d->ny, d->nxt, d->vs, d->P, d->cour,
+                                       d->stream));
+    } else {
+        HB_CU(hb::launch_courant(d->A, d->nx, d->ny, d->nxt, d->vs, d->P, d->cour, d->stream));
+    }
     d->launches += 1;
     d->cour_valid = true;
     return HB_OK;

@@ -234,6 +234,12 @@ long long hydro_b200_batch_arena_free(hb_batch *b);
  * or arena space is free (HB_ERR_NOMEM). */
 int hydro_b200_batch_add(hb_batch *b, const hydroparam_t *H, const double *host, double tend,
                          int nstepmax);
+/* Resume a checkpoint (state downloaded with hydro_b200_batch_download, clock
+ * read with hydro_b200_batch_status): clock from H->t and H->nstep, and dt,
+ * the step size in force (used when H->nstep is odd, as main.c keeps the dt
+ * of an even step for the odd step after it). */
+int hydro_b200_batch_add_resume(hb_batch *b, const hydroparam_t *H, const double *host, double dt,
+                                double tend, int nstepmax);
 /* The same with the initial state written on the device: a single blast
  * (density rho, zero momenta, energy e_bg, and e_blast in the padded cell
  * (bi, bj); ghost cells 0). */

@@ -124,3 +124,32 @@ def test_arena_budget_admission(product_lib):
     b.remove(got[1])
     assert b.try_add(H, u) >= 0
     b.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("at", [6, 7])
+def test_checkpoint_resume_is_seamless(product_lib, precision, at):
+    """Checkpoint an instance at an even or odd step, drop it, resume it in
+    another batch: the result equals the uninterrupted run bit for bit."""
+    H, u = blast_instance(96, 72, 0.4, 0.6, 1.5, 0.9)
+    ref = Batch(H, capacity=2, arena_bytes=ARENA, precision=precision)
+    s = ref.add(H, u)
+    ref.steps(13)
+    want = ref.download(s)
+    ref.close()
+    a = Batch(H, capacity=4, arena_bytes=ARENA, precision=precision)
+    for Ho, uo in mix_of(3, 31):
+        a.add(Ho, uo)
+    s = a.add(H, u)
+    a.steps(at)
+    ck = a.checkpoint(s)
+    a.remove(s)
+    a.close()
+    assert ck["nstep"] == at
+    b = Batch(H, capacity=4, arena_bytes=ARENA, precision=precision)
+    b.add(*mix_of(1, 32)[0])
+    s2 = b.resume(ck)
+    b.steps(13 - at)
+    assert b.status(s2)["nstep"] == 13
+    assert bitwise_equal(b.download(s2), want)
+    b.close()
