@@ -29,13 +29,13 @@
 namespace hb {
 
 template <int DIR, bool UNIT>
-__global__ void __launch_bounds__(kSweepThreads)
+__global__ void __launch_bounds__(kSweepThreads, DIR == 2 ? kFp64MarchMinBlocks : 1)
 sweep_kernel(const SweepArgs a, const Phys P) {
     sweep_body<DIR, ExactStages<UNIT>>(a, P);
 }
 
 template <bool UNIT>
-__global__ void __launch_bounds__(kCellThreads)
+__global__ void __launch_bounds__(kCellThreads, kFp64CellMinBlocks)
 xcell_kernel(const SweepArgs a, const Phys P) {
     xcell_body<ExactStages<UNIT>>(a, P);
 }

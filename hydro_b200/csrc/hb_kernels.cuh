@@ -52,6 +52,15 @@ cudaError_t launch_sweep(int dir, const SweepArgs& a, const Phys& P, cudaStream_
 int sweep_blocks_per_sm(int dir, bool unit_slope);
 // The x sweep with one cell per lane (hb_march.cuh xcell_body): FP64 and mixed.
 constexpr int kCellThreads = 64;
+
+// Minimum resident CTAs per SM the sweep kernels are compiled for (register
+// caps).  The FP64 kernels are latency-bound: more resident warps beat the
+// few register spills the caps cause (measured at 4096^2: marching y sweep
+// 1.66 -> 1.49 ms, cell-per-lane x sweep 1.63 -> 1.56 ms).  The mixed marching
+// sweep keeps its registers for the next-cell prefetch and is not capped.
+constexpr int kFp64MarchMinBlocks = 16;
+constexpr int kFp64CellMinBlocks = 18;
+constexpr int kMixedCellMinBlocks = 18;
 constexpr int kCellWarpOut = 28;  // outputs per warp of the cell-per-lane x sweep
 cudaError_t launch_xcell(const SweepArgs& a, const Phys& P, cudaStream_t s);
 cudaError_t launch_xcell_mixed(const SweepArgs& a, const Phys& P, cudaStream_t s);

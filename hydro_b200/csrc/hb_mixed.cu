@@ -14,7 +14,7 @@ sweep_mixed_kernel(const SweepArgs a, const Phys P) {
     sweep_body<DIR, MixedStages>(a, P);
 }
 
-__global__ void __launch_bounds__(kCellThreads)
+__global__ void __launch_bounds__(kCellThreads, kMixedCellMinBlocks)
 xcell_mixed_kernel(const SweepArgs a, const Phys P) {
     xcell_body<MixedStages>(a, P);
 }

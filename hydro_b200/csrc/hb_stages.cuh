@@ -81,10 +81,13 @@ __device__ __forceinline__ double slope1(double st, double qm, double q0, double
         drgt = st * (qp - q0);
         dcen = 0.5 * (dlft + drgt) / st;
     }
-    double dsgn = (dcen > 0.0) ? 1.0 : -1.0;
-    int llftrgt = ((dlft * drgt) <= 0.0);
-    double t1 = cfmin(fabs(dlft), fabs(drgt));
-    return dsgn * cfmin((double)(1 - llftrgt) * t1, fabs(dcen));
+    // dsgn * fmin((1 - llftrgt) * t1, |dcen|) of the reference, written as a
+    // select: for finite slopes (1 - llftrgt) * t1 is t1 or +0, fmin(+0, x >= 0)
+    // is +0, and (-1) * m is -m exactly, so the bits are the same.
+    const bool llftrgt = (dlft * drgt) <= 0.0;
+    const double t1 = cfmin(fabs(dlft), fabs(drgt));
+    const double m = llftrgt ? 0.0 : cfmin(t1, fabs(dcen));
+    return (dcen > 0.0) ? m : -m;
 }
 
 template <bool UNIT>
