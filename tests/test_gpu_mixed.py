@@ -45,6 +45,24 @@ def test_mixed_l1_error_against_fp64(product_lib, nx, ny, tc, nsteps, noise):
     assert np.all(np.isfinite(mix))
 
 
+def test_mixed_full_size_noisy_corner_8192(product_lib, capsys):
+    """The mixed-precision workload at its full size: 8192^2, corner blast,
+    density times 1 + 0.01 U(-1, 1), 500 steps, against the FP64 path on the
+    same input.  The errors are printed for the record."""
+    H = make_params(8192, 8192, testcase=1)
+    u0 = init_noisy_blast(H, 20261203, testcase=1)
+    ref, tref = run(H, u0, 500, "fp64")
+    mix, tmix = run(H, u0, 500, "mixed")
+    del u0
+    err = field_errors(mix, ref)
+    with capsys.disabled():
+        print(f"\n8192^2 noisy corner, 500 steps, mixed vs fp64: {err}, t {tmix!r} vs {tref!r}")
+    assert err["rho"]["l1_rel"] <= L1_BOUND, err
+    assert err["E"]["l1_rel"] <= L1_BOUND, err
+    assert abs(tmix - tref) <= 1e-5 * tref
+    assert np.all(np.isfinite(mix[:, 2:-2, 2:-2]))
+
+
 def test_mixed_conserves_mass_and_energy(product_lib):
     H = make_params(300, 300, testcase=0)
     u0 = init_state(H, 0)
