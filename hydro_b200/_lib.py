@@ -121,6 +121,10 @@ SIGNATURES = [
     ("hydro_b200_domain_godunov", C.c_int, [_D, C.c_int, C.c_double, C.c_int]),
     ("hydro_b200_domain_make_boundary", C.c_int, [_D, C.c_int]),
     ("hydro_b200_domain_courant", C.c_int, [_D, _DP, _DP]),
+    ("hydro_b200_domain_sweep", C.c_int, [_D, C.c_int, C.c_int, C.c_double, C.c_int]),
+    ("hydro_b200_domain_halo_count", C.c_longlong, [_D, C.c_int]),
+    ("hydro_b200_domain_halo_pack", C.c_int, [_D, C.c_int, C.c_int, C.c_int, C.c_void_p]),
+    ("hydro_b200_domain_halo_unpack", C.c_int, [_D, C.c_int, C.c_int, C.c_void_p]),
     ("hydro_b200_domain_set_clock", C.c_int, [_D, C.c_double, C.c_int, C.c_double]),
     ("hydro_b200_domain_launch_steps", C.c_int, [_D, C.c_int, C.c_int, C.c_double]),
     ("hydro_b200_domain_get_clock", C.c_int, [_D, _DP, C.POINTER(C.c_int), _DP]),

@@ -143,6 +143,49 @@ cudaError_t launch_boundary(double* u, int idim, int nx, int ny, int nxt, int ny
     return cudaGetLastError();
 }
 
+// Halo strips of a domain split (make_boundary.c:48-52, mpibounds.c:165-310):
+// the two interior lines next to one side, for the interior lines of the other
+// direction, packed as [var][line][2] (idim 1: columns, per interior row) or
+// [var][2][line] (idim 2: rows, per interior column).  Pack reads interior
+// cells of `u`; unpack writes the ghost cells of the same side.  One thread per
+// value; the index map is the same both ways, so unpacking a neighbour's pack
+// of the opposite side puts its cells where a single grid would have them.
+__global__ void halo_kernel(double* u, double* buf, int pack, int idim, int side, int nx, int ny,
+                            int nxt, long long vs) {
+    const int nlines = (idim == 1) ? ny : nx;
+    const int total = 8 * nlines;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    int v, l, c;
+    if (idim == 1) {
+        c = t & 1;
+        l = (t >> 1) % nlines;
+        v = (t >> 1) / nlines;
+    } else {
+        l = t % nlines;
+        c = (t / nlines) & 1;
+        v = (t / nlines) >> 1;
+    }
+    const int nl = (idim == 1) ? nx : ny;
+    // interior source line and ghost destination line along the sweep axis
+    const int k_in = side == 0 ? 2 + c : nl + c;
+    const int k_gh = side == 0 ? c : nl + 2 + c;
+    const int k = pack ? k_in : k_gh;
+    const long long at = (idim == 1) ? (long long)nxt * (l + 2) + k : (long long)nxt * k + (l + 2);
+    if (pack)
+        buf[t] = u[at + v * vs];
+    else
+        u[at + v * vs] = buf[t];
+}
+
+cudaError_t launch_halo(double* u, double* buf, int pack, int idim, int side, int nx, int ny,
+                        int nxt, long long vs, cudaStream_t s) {
+    const int nlines = (idim == 1) ? ny : nx;
+    const int threads = 8 * nlines;
+    halo_kernel<<<(threads + 255) / 256, 256, 0, s>>>(u, buf, pack, idim, side, nx, ny, nxt, vs);
+    return cudaGetLastError();
+}
+
 // main.c:349-392 on the device: on even steps dt = courant_factor*dx /
 // MAX(cournox, MAX(cournoy, smallc)), halved at step 0; stops the clock once
 // t >= tend or nstep >= nstepmax.  Resets the Courant accumulators for the

@@ -346,6 +346,63 @@ extern "C" int hydro_b200_domain_godunov(hb_domain* d, int idim, double dt, int 
     return domain_step(d, idim, dt, nullptr, fuse_courant != 0);
 }
 
+// One sweep of a step, for drivers that act between the two sweeps (a domain
+// split exchanging halos, mpibounds.c:165-310 called from make_boundary.c:48).
+// Stage 0 is the step's first sweep (A -> B), stage 1 the second (B -> A).
+extern "C" int hydro_b200_domain_sweep(hb_domain* d, int stage, int idim, double dt,
+                                       int fuse_courant) {
+    if (!d) return set_error(HB_ERR_ARG, "null domain");
+    if (idim != 1 && idim != 2) return set_error(HB_ERR_ARG, "idim=%d: expected 1 or 2", idim);
+    if (stage != 0 && stage != 1) return set_error(HB_ERR_ARG, "stage=%d: expected 0 or 1", stage);
+    if (stage == 0 && fuse_courant)
+        return set_error(HB_ERR_ARG, "the Courant reduction fuses into the second sweep only");
+    if (fuse_courant) HB_CU(cudaMemsetAsync(d->cour, 0, kCourBytes, d->stream));
+    SweepArgs a = stage == 0 ? sweep_args(d, idim, d->A, d->B, nullptr, dt, nullptr)
+                             : sweep_args(d, idim, d->B, d->A, nullptr, dt,
+                                          fuse_courant ? d->cour : nullptr);
+    const int rc = launch_sweep_timed(d, idim, a);
+    if (rc) return rc;
+    d->cour_valid = stage == 1 && fuse_courant;
+    return HB_OK;
+}
+
+static int halo_args(hb_domain* d, int idim, int side, const void* buf) {
+    if (!d) return set_error(HB_ERR_ARG, "null domain");
+    if (idim != 1 && idim != 2) return set_error(HB_ERR_ARG, "idim=%d: expected 1 or 2", idim);
+    if (side != 0 && side != 1) return set_error(HB_ERR_ARG, "side=%d: expected 0 or 1", side);
+    if (!buf) return set_error(HB_ERR_ARG, "null halo buffer");
+    return HB_OK;
+}
+
+extern "C" long long hydro_b200_domain_halo_count(hb_domain* d, int idim) {
+    if (!d || (idim != 1 && idim != 2)) return 0;
+    return 8ll * (idim == 1 ? d->ny : d->nx);
+}
+
+extern "C" int hydro_b200_domain_halo_pack(hb_domain* d, int stage, int idim, int side,
+                                           double* dst) {
+    int rc = halo_args(d, idim, side, dst);
+    if (rc) return rc;
+    if (stage != 0 && stage != 1) return set_error(HB_ERR_ARG, "stage=%d: expected 0 or 1", stage);
+    // Before the first sweep the state is A; before the second, the first
+    // sweep's output B holds the interior.
+    HB_CU(hb::launch_halo(stage == 0 ? d->A : d->B, dst, 1, idim, side, d->nx, d->ny, d->nxt,
+                          d->vs, d->stream));
+    d->launches += 1;
+    return HB_OK;
+}
+
+extern "C" int hydro_b200_domain_halo_unpack(hb_domain* d, int idim, int side,
+                                             const double* src) {
+    int rc = halo_args(d, idim, side, src);
+    if (rc) return rc;
+    // Ghost cells of both sweeps are read from A.
+    HB_CU(hb::launch_halo(d->A, const_cast<double*>(src), 0, idim, side, d->nx, d->ny, d->nxt,
+                          d->vs, d->stream));
+    d->launches += 1;
+    return HB_OK;
+}
+
 extern "C" int hydro_b200_domain_set_precision(hb_domain* d, int precision) {
     if (!d) return set_error(HB_ERR_ARG, "null domain");
     if (precision != HB_PREC_FP64 && precision != HB_PREC_MIXED)

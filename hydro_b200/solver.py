@@ -176,6 +176,19 @@ class Domain:
         check(self.lib.hydro_b200_domain_courant(self.h, C.byref(cx), C.byref(cy)))
         return cx.value, cy.value
 
+    # --- one sweep at a time, and halo strips (domain split) ------------------
+    def sweep(self, stage: int, idim: int, dt: float, fuse_courant: bool = False) -> None:
+        check(self.lib.hydro_b200_domain_sweep(self.h, stage, idim, dt, int(fuse_courant)))
+
+    def halo_count(self, idim: int) -> int:
+        return int(self.lib.hydro_b200_domain_halo_count(self.h, idim))
+
+    def halo_pack(self, stage: int, idim: int, side: int, dst_ptr: int) -> None:
+        check(self.lib.hydro_b200_domain_halo_pack(self.h, stage, idim, side, dst_ptr))
+
+    def halo_unpack(self, idim: int, side: int, src_ptr: int) -> None:
+        check(self.lib.hydro_b200_domain_halo_unpack(self.h, idim, side, src_ptr))
+
     def set_clock(self, t: float = 0.0, nstep: int = 0, dt: float = 0.0) -> None:
         check(self.lib.hydro_b200_domain_set_clock(self.h, t, nstep, dt))
 
@@ -186,6 +199,13 @@ class Domain:
         t, n, dt = C.c_double(), C.c_int(), C.c_double()
         check(self.lib.hydro_b200_domain_get_clock(self.h, C.byref(t), C.byref(n), C.byref(dt)))
         return t.value, n.value, dt.value
+
+    def get_dts(self, n: int) -> np.ndarray:
+        """dt of steps 0 .. n-1 of the launch-only driver (device record)."""
+        out = np.zeros(max(n, 1), dtype=np.float64)
+        check(self.lib.hydro_b200_domain_get_dts(self.h, out.ctypes.data_as(C.POINTER(C.c_double)),
+                                                 n))
+        return out[:n]
 
     def profile(self, enable: bool = True) -> None:
         check(self.lib.hydro_b200_domain_profile(self.h, int(enable)))

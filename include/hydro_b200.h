@@ -179,6 +179,31 @@ int hydro_b200_domain_synchronize(hb_domain *d);
 int hydro_b200_domain_godunov(hb_domain *d, int idim, double dt, int fuse_courant);
 int hydro_b200_domain_make_boundary(hb_domain *d, int idim);
 int hydro_b200_domain_courant(hb_domain *d, double *cournox, double *cournoy); /* synchronous */
+
+/* Domain split (the reference's MPI build of the same variant: SplitSurface.c,
+ * mpibounds.c:165-310 called from make_boundary.c:48-52 and :125-129, the dt
+ * MPI_Allreduce of main.c:361-372).  A subdomain's sides that face a neighbour
+ * carry boundary type 0 (parametres.c:318-330): their ghost cells are not
+ * filled by make_boundary but received from the neighbour before each sweep.
+ *
+ * hydro_b200_domain_sweep runs ONE sweep of a step: stage 0 is the step's
+ * first sweep (direction idim), stage 1 its second.  A step is
+ * sweep(0, first) then sweep(1, second), the same work as
+ * hydro_b200_domain_godunov; fuse_courant (stage 1 only) reduces the Courant
+ * maxima of the result for the next hydro_b200_domain_courant.
+ *
+ * Halo strips: hydro_b200_domain_halo_count(d, idim) doubles, the two
+ * interior lines next to side (0 = left/down, 1 = right/up) of direction idim
+ * over the interior lines of the other direction.  pack reads the state the
+ * given stage's sweep reads (stage 0: the step's input; stage 1: the first
+ * sweep's output); unpack writes the ghost cells of that side.  A neighbour's
+ * strip of side 1-s unpacked at side s places its cells exactly where a single
+ * grid holds them.  Buffers are device pointers; all three run asynchronously
+ * on the domain's stream. */
+int hydro_b200_domain_sweep(hb_domain *d, int stage, int idim, double dt, int fuse_courant);
+long long hydro_b200_domain_halo_count(hb_domain *d, int idim);
+int hydro_b200_domain_halo_pack(hb_domain *d, int stage, int idim, int side, double *dst);
+int hydro_b200_domain_halo_unpack(hb_domain *d, int idim, int side, const double *src);
 /* Launch-only driver (asynchronous; same semantics as hydro_b200_run). */
 int hydro_b200_domain_set_clock(hb_domain *d, double t, int nstep, double dt);
 int hydro_b200_domain_launch_steps(hb_domain *d, int nsteps, int nstepmax, double tend);

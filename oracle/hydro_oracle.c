@@ -339,23 +339,26 @@ static void sweep_line(const orc_param_t *P, int idim, int line, double dtdx, do
     }
 }
 
+/* One sweep of hydro_godunov.c:74-139: make_boundary for direction idim, then
+ * every line of that direction. */
+void orc_sweep(const orc_param_t *P, int idim, double dt, double *uold) {
+    int nmax = (P->nx > P->ny ? P->nx : P->ny) + 4;
+    double dtdx = dt / P->dx;
+    orc_make_boundary(P, idim, uold);
+    int nlines = (idim == 1) ? P->ny : P->nx;
+    int n = (idim == 1) ? P->nx + 4 : P->ny + 4;
+#pragma omp parallel
+    {
+        double *work = (double *)malloc(sizeof(double) * 4 * 8 * (size_t)nmax + 64);
+#pragma omp for schedule(static)
+        for (int l = 0; l < nlines; l++) sweep_line(P, idim, l + XL, dtdx, uold, work, n);
+        free(work);
+    }
+}
+
 /* hydro_godunov.c:70-139: two sweeps, order x->y for idim 1, y->x for 2. */
 void orc_godunov(const orc_param_t *P, int idimStart, double dt, double *uold) {
-    int nmax = (P->nx > P->ny ? P->nx : P->ny) + 4;
-    for (int ii = 0; ii < 2; ii++) {
-        int idim = (idimStart - 1 + ii) % 2 + 1;
-        double dtdx = dt / P->dx;
-        orc_make_boundary(P, idim, uold);
-        int nlines = (idim == 1) ? P->ny : P->nx;
-        int n = (idim == 1) ? P->nx + 4 : P->ny + 4;
-#pragma omp parallel
-        {
-            double *work = (double *)malloc(sizeof(double) * 4 * 8 * (size_t)nmax + 64);
-#pragma omp for schedule(static)
-            for (int l = 0; l < nlines; l++) sweep_line(P, idim, l + XL, dtdx, uold, work, n);
-            free(work);
-        }
-    }
+    for (int ii = 0; ii < 2; ii++) orc_sweep(P, (idimStart - 1 + ii) % 2 + 1, dt, uold);
 }
 
 /* compute_deltat.c:31-77 with ComputeQEforRow.c:31-47, equation_of_state.c

@@ -75,6 +75,7 @@ def oracle_lib():
             lib.orc_init.restype = C.c_int
             lib.orc_make_boundary.argtypes = [_P, C.c_int, _DP]
             lib.orc_godunov.argtypes = [_P, C.c_int, C.c_double, _DP]
+            lib.orc_sweep.argtypes = [_P, C.c_int, C.c_double, _DP]
             lib.orc_courant.argtypes = [_P, _DP, C.POINTER(C.c_double), C.POINTER(C.c_double)]
             lib.orc_courant.restype = C.c_double
             lib.orc_run.argtypes = [_P, _DP, C.c_int, C.c_double, C.c_void_p,
@@ -129,6 +130,11 @@ def init_state(p: OrcParam, testcase: int) -> np.ndarray:
 
 def godunov(p: OrcParam, idim: int, dt: float, u: np.ndarray) -> None:
     oracle_lib().orc_godunov(C.byref(p), idim, dt, u)
+
+
+def sweep(p: OrcParam, idim: int, dt: float, u: np.ndarray) -> None:
+    """make_boundary(idim) and one sweep (hydro_godunov.c:74-139)."""
+    oracle_lib().orc_sweep(C.byref(p), idim, dt, u)
 
 
 def make_boundary(p: OrcParam, idim: int, u: np.ndarray) -> None:
