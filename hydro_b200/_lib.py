@@ -125,6 +125,9 @@ SIGNATURES = [
     ("hydro_b200_domain_halo_count", C.c_longlong, [_D, C.c_int]),
     ("hydro_b200_domain_halo_pack", C.c_int, [_D, C.c_int, C.c_int, C.c_int, C.c_void_p]),
     ("hydro_b200_domain_halo_unpack", C.c_int, [_D, C.c_int, C.c_int, C.c_void_p]),
+    ("hydro_b200_vtk_base64_len", C.c_longlong, [C.c_int, C.c_int]),
+    ("hydro_b200_domain_vtk_base64", C.c_int, [_D, C.c_int, C.c_void_p, C.c_longlong]),
+    ("vtkfile", None, [C.c_int, HydroParam, _V]),
     ("hydro_b200_domain_set_clock", C.c_int, [_D, C.c_double, C.c_int, C.c_double]),
     ("hydro_b200_domain_launch_steps", C.c_int, [_D, C.c_int, C.c_int, C.c_double]),
     ("hydro_b200_domain_get_clock", C.c_int, [_D, _DP, C.POINTER(C.c_int), _DP]),

@@ -73,6 +73,8 @@ cudaError_t launch_courant_mixed(const double* u, int nx, int ny, int nxt, long 
                                  const Phys& P, unsigned long long* cour, cudaStream_t s);
 cudaError_t launch_boundary(double* u, int idim, int nx, int ny, int nxt, int nyt, long long vs,
                             int bnd_lo, int bnd_hi, cudaStream_t s);
+cudaError_t launch_vtk_base64(const double* var_plane, int nx, int ny, int nxt,
+                              unsigned char* out, cudaStream_t s);
 cudaError_t launch_halo(double* u, double* buf, int pack, int idim, int side, int nx, int ny,
                         int nxt, long long vs, cudaStream_t s);
 cudaError_t launch_clock_begin(DevClock* c, unsigned long long* cour, double courant_factor,

@@ -99,6 +99,8 @@ struct hb_domain {
     std::vector<int> ev_dir;
     double prof_ms[2] = {0.0, 0.0};
     long long prof_n[2] = {0, 0};
+    unsigned char* b64 = nullptr;  // VTK output text of one variable (hb_output.cu)
+    size_t b64_cap = 0;
 };
 
 static int validate(const hydroparam_t* H) {
@@ -154,6 +156,7 @@ extern "C" void hydro_b200_domain_destroy(hb_domain* d) {
     cudaFree(d->cour);
     cudaFree(d->clk);
     cudaFree(d->dts);
+    cudaFree(d->b64);
     if (d->stream) cudaStreamDestroy(d->stream);
     delete d;
 }
@@ -400,6 +403,28 @@ extern "C" int hydro_b200_domain_halo_unpack(hb_domain* d, int idim, int side,
     HB_CU(hb::launch_halo(d->A, const_cast<double*>(src), 0, idim, side, d->nx, d->ny, d->nxt,
                           d->vs, d->stream));
     d->launches += 1;
+    return HB_OK;
+}
+
+// vtkfile.c:262-280 on the device: variable `var` of the interior as floats,
+// base64-encoded, into host memory (hydro_b200_vtk_base64_len(nx, ny) bytes).
+extern "C" int hydro_b200_domain_vtk_base64(hb_domain* d, int var, char* host_out,
+                                            long long cap) {
+    if (!d || !host_out) return set_error(HB_ERR_ARG, "null argument");
+    if (var < 0 || var > 3) return set_error(HB_ERR_ARG, "var=%d: expected 0..3", var);
+    const long long n = hydro_b200_vtk_base64_len(d->nx, d->ny);
+    if (cap < n) return set_error(HB_ERR_ARG, "output buffer of %lld bytes < %lld", cap, n);
+    if (d->b64_cap < (size_t)n + 16) {
+        cudaFree(d->b64);
+        d->b64 = nullptr;
+        d->b64_cap = 0;
+        HB_CU(cudaMalloc(&d->b64, (size_t)n + 16));
+        d->b64_cap = (size_t)n + 16;
+    }
+    HB_CU(hb::launch_vtk_base64(d->A + var * d->vs, d->nx, d->ny, d->nxt, d->b64, d->stream));
+    d->launches += 1;
+    HB_CU(cudaMemcpyAsync(host_out, d->b64, (size_t)n, cudaMemcpyDeviceToHost, d->stream));
+    HB_CU(cudaStreamSynchronize(d->stream));
     return HB_OK;
 }
 
@@ -703,6 +728,15 @@ extern "C" void make_boundary(int idim, const hydroparam_t H, hydrovar_t* Hv) {
     if (sync_each_call()) {
         if (hydro_b200_domain_download(d, Hv->uold) == HB_OK) hydro_b200_domain_synchronize(d);
     }
+}
+
+int hb_vtk_write(hb_domain* d, int step, const hydroparam_t* H);  // hb_output.cu
+
+// vtkfile.h: the reference's VTK output, written from the device mirror.
+extern "C" void vtkfile(int step, const hydroparam_t H, hydrovar_t* Hv) {
+    hb_domain* d = mirror_for(&H, Hv);
+    if (!d) return;
+    if (hb_vtk_write(d, step, &H) != HB_OK && strict_mode()) abort();
 }
 
 extern "C" void compute_deltat_init_mem(const hydroparam_t H, hydrowork_t* Hw,

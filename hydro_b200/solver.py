@@ -189,6 +189,13 @@ class Domain:
     def halo_unpack(self, idim: int, side: int, src_ptr: int) -> None:
         check(self.lib.hydro_b200_domain_halo_unpack(self.h, idim, side, src_ptr))
 
+    def vtk_base64(self, var: int) -> bytes:
+        """The VTK writer's base64 payload of variable `var` (0..3)."""
+        n = int(self.lib.hydro_b200_vtk_base64_len(self.H.nx, self.H.ny))
+        buf = C.create_string_buffer(n)
+        check(self.lib.hydro_b200_domain_vtk_base64(self.h, var, buf, n))
+        return buf.raw[:n]
+
     def set_clock(self, t: float = 0.0, nstep: int = 0, dt: float = 0.0) -> None:
         check(self.lib.hydro_b200_domain_set_clock(self.h, t, nstep, dt))
 

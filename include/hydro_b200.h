@@ -123,6 +123,15 @@ void compute_deltat(real_t *dt, const hydroparam_t H, hydrowork_t *Hw, hydrovar_
  * ghost layers of direction idim on the device mirror. */
 void make_boundary(int idim, const hydroparam_t H, hydrovar_t *Hv);
 
+/* Replaces vtkfile.c:140-352 (declared vtkfile.h:3): the same files
+ * (Dep/XXXX/YY/Hydro_<pe>_<step>.vtr, the .pvtr header on rank 0, Hydro.pvd),
+ * byte for byte, written from the device mirror of Hv->uold: the float
+ * conversion and base64 encoding run on the GPU, so no host copy of the state
+ * is needed.  Link it by leaving vtkfile.c out of the reference's objects.
+ * Unlike the reference it creates the directories on every rank and has no
+ * MPI barriers. */
+void vtkfile(int step, const hydroparam_t H, hydrovar_t *Hv);
+
 /* Replace compute_deltat.c:15-29 (declared compute_deltat.h:7-8).  init_mem
  * allocates nothing (the device path needs no host work arrays) and sets the
  * pointers to NULL; clean_mem copies every device mirror back to its host
@@ -202,6 +211,12 @@ int hydro_b200_domain_courant(hb_domain *d, double *cournox, double *cournoy); /
  * on the domain's stream. */
 int hydro_b200_domain_sweep(hb_domain *d, int stage, int idim, double dt, int fuse_courant);
 long long hydro_b200_domain_halo_count(hb_domain *d, int idim);
+/* VTK payload of one variable (0..3 = rho, rho u, rho v, E): the interior in
+ * row order as floats (C's (float) cast), base64-encoded as vtkfile.c:262-280
+ * does, written to host memory; hydro_b200_vtk_base64_len(nx, ny) bytes (no
+ * terminator; the 8-character length header is not included). */
+long long hydro_b200_vtk_base64_len(int nx, int ny);
+int hydro_b200_domain_vtk_base64(hb_domain *d, int var, char *host_out, long long cap);
 int hydro_b200_domain_halo_pack(hb_domain *d, int stage, int idim, int side, double *dst);
 int hydro_b200_domain_halo_unpack(hb_domain *d, int idim, int side, const double *src);
 /* Launch-only driver (asynchronous; same semantics as hydro_b200_run). */

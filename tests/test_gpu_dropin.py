@@ -1,6 +1,7 @@
 """The unmodified reference driver (main.c, parameter reader, init, VTK
 writer) linked against libhydro_b200.so in place of its hot path
-(oracle/_ref/hydro_dropin) against the reference application itself
+(oracle/_ref/hydro_dropin), and with the library's VTK writer too
+(oracle/_ref/hydro_dropin_vtk), against the reference application itself
 (oracle/_ref/hydro): same step lines and byte-identical VTK output files.
 Skipped where the reference could not be compiled."""
 import filecmp
@@ -36,26 +37,55 @@ niter_riemann=10
 """
 
 
-@pytest.mark.skipif(not (os.path.exists(os.path.join(REF, "hydro_dropin"))
-                         and os.path.exists(os.path.join(REF, "hydro"))),
-                    reason="reference application not compiled here")
-def test_reference_driver_runs_on_the_gpu_path(tmp_path, product_lib):
+# hydro_dropin: the reference's own vtkfile.c reads the host array, which the
+# library copies back after every step (HYDRO_B200_SYNC=1).
+# hydro_dropin_vtk: the library's vtkfile writes from the device state; the
+# host array is never updated during the run.
+@pytest.mark.parametrize("name,sync", [("hydro_dropin", "1"), ("hydro_dropin_vtk", "0")])
+def test_reference_driver_runs_on_the_gpu_path(tmp_path, product_lib, name, sync):
+    if not (os.path.exists(os.path.join(REF, name)) and os.path.exists(os.path.join(REF, "hydro"))):
+        pytest.skip("reference application not compiled here")
     outs = {}
-    for name in ("hydro", "hydro_dropin"):
-        d = tmp_path / name
+    for exe, env_sync in (("hydro", "0"), (name, sync)):
+        d = tmp_path / exe
         d.mkdir()
         (d / "in.nml").write_text(NML)
-        env = dict(os.environ, HYDRO_B200_SYNC="1", OMP_NUM_THREADS="4")
-        r = subprocess.run([os.path.join(REF, name), "-i", "in.nml"], cwd=d, env=env,
+        env = dict(os.environ, HYDRO_B200_SYNC=env_sync, OMP_NUM_THREADS="4")
+        r = subprocess.run([os.path.join(REF, exe), "-i", "in.nml"], cwd=d, env=env,
                            capture_output=True, text=True, timeout=300)
         assert r.returncode == 0, r.stderr[-2000:]
         steps = re.findall(r"--> step=\s*(\d+),\s*(\S+),\s*(\S+)", r.stdout)
         assert len(steps) == 60
-        outs[name] = (d, steps)
-    assert outs["hydro"][1] == outs["hydro_dropin"][1]
-    a, b = outs["hydro"][0], outs["hydro_dropin"][0]
+        outs[exe] = (d, steps)
+    assert outs["hydro"][1] == outs[name][1]
+    a, b = outs["hydro"][0], outs[name][0]
     files = sorted(os.path.relpath(os.path.join(dp, f), a)
-                   for dp, _, fs in os.walk(a) for f in fs if f.endswith(".vtr"))
-    assert len(files) >= 3
+                   for dp, _, fs in os.walk(a) for f in fs
+                   if f.endswith((".vtr", ".pvtr", ".pvd")))
+    assert sum(f.endswith(".vtr") for f in files) >= 3
     for f in files:
         assert filecmp.cmp(os.path.join(a, f), os.path.join(b, f), shallow=False), f
+
+
+@pytest.mark.parametrize("nx,ny", [(37, 29), (33, 17), (34, 17), (250, 125)])
+def test_vtk_base64_payload_matches_float_cast(product_lib, nx, ny):
+    """The device encoder against numpy's float32 cast (round to nearest even,
+    as C's (float) cast) and the standard base64 of the bytes."""
+    import base64
+
+    import numpy as np
+
+    from hydro_b200 import Domain, make_params
+    H = make_params(nx, ny)
+    rng = np.random.default_rng(nx * ny)
+    u = rng.standard_normal((4, ny + 4, nx + 4)) * np.exp(rng.uniform(-100, 100, (4, ny + 4, nx + 4)))
+    u[0, 2, 2] = 1e-41  # a float subnormal after the cast
+    u[1, 3, 3] = -0.0
+    u[2, 2, 3] = 1.0000000596046448  # a tie between two floats
+    d = Domain(H)
+    d.upload(u)
+    for v in range(4):
+        with np.errstate(over="ignore"):  # values beyond float range become inf, as in C
+            want = base64.b64encode(u[v, 2:-2, 2:-2].astype(np.float32).tobytes())
+        assert d.vtk_base64(v) == want, v
+    d.close()
