@@ -183,6 +183,74 @@ def dom_state_after(H, u0, nsteps, precision):
     return u
 
 
+def run_vtk_form(H, u):
+    """One VTK output of the state `u` (the output path, vtkfile.c:140-352):
+    the library's vtkfile, which encodes on the GPU from the device mirror.
+    Its CPU baseline is the reference's own vtkfile.c (oracle/_ref), fed by a
+    device-to-host copy of the state (what a host writer needs when the state
+    lives on the GPU).  Both write the same files, compared byte for byte, to
+    local temporary directories; wall time of one call each."""
+    import ctypes as C
+    import filecmp
+    import shutil
+    import tempfile
+
+    from hydro_b200 import HydroRun
+    from hydro_b200._lib import check
+    run = HydroRun(H, u.copy())
+    run.sync_to_device()  # the state is resident before the timed call
+    lib = run.lib
+    out = {"unit": "ms per output", "cells": H.nx * H.ny,
+           "text_bytes": 4 * int(lib.hydro_b200_vtk_base64_len(H.nx, H.ny))}
+    cwd = os.getcwd()
+    dirs = [tempfile.mkdtemp(prefix="hb_vtk_"), tempfile.mkdtemp(prefix="hb_vtk_")]
+    try:
+        os.chdir(dirs[0])
+        lib.vtkfile(1, H, C.byref(run.Hv))  # first call: buffers, directories
+        t0 = time.perf_counter()
+        lib.vtkfile(1, H, C.byref(run.Hv))
+        out["value"] = round((time.perf_counter() - t0) * 1e3, 2)
+        check()
+        try:
+            from oracle import oracle as O
+            if not O.ref_available():
+                raise RuntimeError("reference not compiled")
+            ref = O.RefState(O.make_param(H.nx, H.ny), 0)
+            os.chdir(dirs[1])
+            devnull = os.open(os.devnull, os.O_WRONLY)
+            saved = os.dup(1)
+            try:
+                sys.stdout.flush()
+                os.dup2(devnull, 1)  # vtkfile.c prints the decomposition once
+                t0 = time.perf_counter()
+                ref.set(run.sync_to_host())
+                ref.vtkfile(1)
+                ref_ms = (time.perf_counter() - t0) * 1e3
+            finally:
+                os.dup2(saved, 1)
+                os.close(saved)
+                os.close(devnull)
+            ref.close()
+            names = [os.path.relpath(os.path.join(dp, f), dirs[0])
+                     for dp, _, fs in os.walk(dirs[0]) for f in fs]
+            out["files_identical"] = all(filecmp.cmp(os.path.join(dirs[0], n),
+                                                     os.path.join(dirs[1], n), shallow=False)
+                                         for n in names)
+            out["cpu_baseline"] = {"value": round(ref_ms, 2), "unit": "ms per output",
+                                   "cores": 1, "kind": "reference",
+                                   "sample": "device-to-host copy of the state, then "
+                                             "vtkfile.c on it (one output)"}
+        except Exception as e:  # the reference build is optional here
+            out["cpu_baseline"] = None
+            out["cpu_baseline_note"] = str(e)[:200]
+    finally:
+        os.chdir(cwd)
+        run.close()
+        for d in dirs:
+            shutil.rmtree(d, ignore_errors=True)
+    return out
+
+
 def run_batched_form(device, seed=20261203, n=256, nsteps=100):
     """The batched workload: n seeded instances (sides log-uniform in
     [64, 1024], multiples of 8), mixed precision, nsteps steps each, one
@@ -313,6 +381,7 @@ def main():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-vtk", action="store_true")
     ap.add_argument("--serving-wall", type=float, default=25.0)
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
@@ -418,6 +487,8 @@ def main():
                           "precision": "FP32 stages; FP64 Newton p*, update, Courant"}
         del ref_state, mix_state
 
+    if not args.no_vtk and rank == 0 and world == 1:
+        forms["vtk_output"] = run_vtk_form(H, dom_state_after(H, u0, min(K, 20), "fp64"))
     if not args.no_batched and rank == 0:
         forms["batched"] = run_batched_form(device)
     if not args.no_serving and rank == 0:

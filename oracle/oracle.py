@@ -105,6 +105,7 @@ def ref_lib():
             lib.ref_compute_deltat.restype = C.c_double
             lib.ref_godunov.argtypes = [C.c_void_p, C.c_int, C.c_double]
             lib.ref_make_boundary.argtypes = [C.c_void_p, C.c_int]
+            lib.ref_vtkfile.argtypes = [C.c_void_p, C.c_int]
             lib.ref_run.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_void_p,
                                     C.POINTER(C.c_double), C.POINTER(C.c_double),
                                     C.POINTER(C.c_double)]
@@ -183,6 +184,10 @@ class RefState:
 
     def make_boundary(self, idim: int) -> None:
         self.lib.ref_make_boundary(self.h, idim)
+
+    def vtkfile(self, step: int) -> None:
+        """vtkfile.c on the state, writing into the current directory."""
+        self.lib.ref_vtkfile(self.h, step)
 
     def run(self, nstepmax: int, tend: float = 1e300):
         dts = np.zeros(max(nstepmax, 1), dtype=np.float64)

@@ -21,6 +21,7 @@
 #include "hydro_funcs.h"
 #include "hydro_godunov.h"
 #include "make_boundary.h"
+#include "vtkfile.h"
 
 #include "orc_param.h"
 
@@ -210,4 +211,11 @@ int ref_parse_nml(const char *path, double *out) {
     int n = (int)(sizeof(v) / sizeof(v[0]));
     for (int i = 0; i < n; i++) out[i] = v[i];
     return n;
+}
+
+/* The reference's VTK writer (vtkfile.c:140-352) on the state, into the
+ * current directory; output number `step`. */
+void ref_vtkfile(void *h, int step) {
+    ref_state_t *s = (ref_state_t *)h;
+    vtkfile(step, s->H, &s->Hv);
 }
