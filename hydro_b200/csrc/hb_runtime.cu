@@ -161,32 +161,38 @@ extern "C" void hydro_b200_domain_destroy(hb_domain* d) {
     delete d;
 }
 
-// Segment length of a sweep: the grid has ceil(nlines/64) x ceil(nl/seg) CTAs.
-// Pick seg so that the CTA count fills whole waves of the resident slots (no
-// partly filled last wave), while keeping seg >= 24: a segment recomputes a
-// 4-cell halo, about 1.6/seg of the work.
-static int choose_seg(int nlines, int nl, int slots) {
-    const int groups = (nlines + hb::kSweepThreads - 1) / hb::kSweepThreads;
-    int best = 64;
+// Segment length of a sweep: the grid has ceil(nlines/64) x ceil(nl/seg) CTAs,
+// each marching one segment plus a 4-cell halo.  Measured on B200:
+//  - a grid with fewer CTAs than resident slots runs them all at once, so its
+//    time is one segment's: shorter segments (down to 8 cells) help until the
+//    grid fills a wave (512^2 FP64 y sweep: 0.41 ms at seg 64, 0.09 ms at 8);
+//  - otherwise the length that fills whole waves best, weighed against the
+//    halo (about 1.6/seg of the work), capped at `cap`: the FP64 y sweep runs
+//    faster with several waves of ~32-cell segments than with one wave of
+//    long ones (4096^2: 1.43 against 1.49 ms; 8192^2: 5.41 against 5.61 ms).
+static int choose_seg(int nlines, int nl, int slots, int cap) {
+    const long long groups = (nlines + hb::kSweepThreads - 1) / hb::kSweepThreads;
+    auto ctas = [&](int seg) { return groups * ((nl + seg - 1) / seg); };
+    if (ctas(24) < slots) {
+        int seg = 24;
+        while (seg > 8 && ctas(seg) < slots) seg -= 2;
+        return seg;
+    }
+    int best = 24;
     double best_score = -1.0;
-    for (int w = 1; w <= 64; w++) {
-        const int nseg_want = (int)((long long)w * slots / groups);
-        if (nseg_want < 1) continue;
-        // Even lengths keep every thread's first cell 16-byte aligned for the
-        // x sweep's vector loads.
-        const int seg = (((nl + nseg_want - 1) / nseg_want) + 1) & ~1;
-        if (seg < 24) break;
-        const int nseg = (nl + seg - 1) / seg;
-        const long long ctas = (long long)groups * nseg;
-        const long long waves = (ctas + slots - 1) / slots;
-        const double fill = (double)ctas / (double)(waves * slots);
+    // Even lengths keep every thread's first cell 16-byte aligned for the x
+    // sweep's vector loads.
+    for (int seg = 24; seg <= nl + 1 && seg <= 8192; seg += 2) {
+        const long long n = ctas(seg);
+        const long long waves = (n + slots - 1) / slots;
+        const double fill = (double)n / (double)(waves * slots);
         const double score = fill / (1.0 + 1.6 / seg);
         if (score > best_score + 1e-9) {
             best_score = score;
             best = seg;
         }
     }
-    return best;
+    return best < cap ? best : cap;
 }
 
 static int domain_alloc(hb_domain* d) {
@@ -201,8 +207,9 @@ static int domain_alloc(hb_domain* d) {
                                    ? hb::sweep_blocks_per_sm(dir, d->P.unit_slope != 0)
                                    : hb::sweep_mixed_blocks_per_sm(dir);
             const int slots = d->sm_count * per_sm;
-            d->seg[prec][dir] =
-                dir == 1 ? choose_seg(d->ny, d->nx, slots) : choose_seg(d->nx, d->ny, slots);
+            const int cap = (prec == HB_PREC_FP64 && dir == 2) ? 32 : 1 << 30;
+            d->seg[prec][dir] = dir == 1 ? choose_seg(d->ny, d->nx, slots, cap)
+                                         : choose_seg(d->nx, d->ny, slots, cap);
         }
     }
     HB_CU(cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking));
