@@ -8,6 +8,13 @@ and retires solves as their clocks pass tend, which frees slots and memory
 for the queue.  Time to solution is measured from arrival (so it includes
 queueing) to the poll that sees the solve finished.
 
+With ``preempt`` on, requests carry a priority: when the head of the waiting
+line cannot be admitted, running solves of lower priority are checkpointed to
+host memory and removed (the reference's Continue.dump restart files,
+CPP/Domain_Prot.cpp:284-411, held in memory) until it fits; they wait with
+their checkpoint and resume bit for bit when memory frees up.  Waiting solves
+are admitted by priority, then arrival.
+
 The loop talks to a backend (``BatchBackend`` for the GPU); the bookkeeping
 is independent of it, so it is tested on the CPU with a simulated backend.
 """
@@ -21,6 +28,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from .batch import Batch, blast_spec, _u01
+from .params import make_params
 
 
 @dataclass
@@ -33,6 +41,7 @@ class Request:
     by: float
     e0: float
     rho: float
+    priority: int = 0
 
     @property
     def cells(self) -> int:
@@ -81,6 +90,24 @@ class BatchBackend:
     def table(self):
         return self.batch.table()
 
+    def checkpoint(self, slot: int) -> dict:
+        return self.batch.checkpoint(slot)
+
+    def fits_after(self, req: Request, ckpt, slots: list) -> bool:
+        """Whether `req` (or its checkpoint) would fit once `slots` are
+        evicted, by free bytes (the arena's first fit may still find it
+        fragmented)."""
+        nx, ny = (req.side, req.side) if ckpt is None else (ckpt["nx"], ckpt["ny"])
+        need = Batch.bytes_needed(make_params(nx, ny))
+        freed = sum(Batch.bytes_needed(self.batch.params[s]) for s in slots)
+        return need <= self.batch.arena_free + freed
+
+    def try_resume(self, ckpt: dict) -> int:
+        return self.batch.resume(ckpt)
+
+    def evict(self, slot: int) -> None:
+        self.batch.remove(slot)
+
     def release(self, slot: int, req: Request) -> None:
         if self.keep_results:
             self.results[req.rid] = self.batch.download(slot)
@@ -100,6 +127,7 @@ class ServeStats:
     queue_samples: list = field(default_factory=list)  # (time s, queued, running)
     chunks: int = 0
     unfinished: int = 0
+    preemptions: int = 0
 
     def summary(self) -> dict:
         lat = np.array([c[1] for c in self.completed]) if self.completed else np.zeros(0)
@@ -115,45 +143,87 @@ class ServeStats:
             "queue_end": q[-1] if q else 0,
             "running_end": self.unfinished,
             "chunks": self.chunks,
+            "preemptions": self.preemptions,
         }
 
 
 class Server:
-    """First-come first-served continuous batching over a backend."""
+    """Continuous batching over a backend: first-come first-served, or by
+    priority with preemption (``preempt``)."""
 
     def __init__(self, backend, chunk_target_s: float = 0.01, max_chunk: int = 256,
-                 clock=time.perf_counter, sleep=time.sleep):
+                 clock=time.perf_counter, sleep=time.sleep, preempt: bool = False):
         self.backend = backend
         self.chunk_target_s = chunk_target_s
         self.max_chunk = max_chunk
         self.clock = clock
         self.sleep = sleep
+        self.preempt = preempt
+
+    def _place(self, req: Request, ckpt) -> int:
+        return self.backend.try_admit(req) if ckpt is None else self.backend.try_resume(ckpt)
+
+    def _admit(self, st, waiting: list, running: dict) -> None:
+        """Admit from the head of `waiting` (entries [request, checkpoint or
+        None, steps counted]) while memory allows.  With preemption, when the
+        head does not fit, evict running solves of lower priority (lowest
+        first, latest arrival first among equals) -- only if evicting them
+        makes room by the backend's estimate."""
+        while waiting:
+            head = waiting[0]
+            req, ckpt, counted = head
+            slot = self._place(req, ckpt)
+            if slot < 0 and self.preempt:
+                victims = sorted((s for s, (r, _) in running.items() if r.priority < req.priority),
+                                 key=lambda s: (running[s][0].priority, -running[s][0].arrival))
+                chosen = []
+                for v in victims:
+                    chosen.append(v)
+                    if self.backend.fits_after(req, ckpt, chosen):
+                        break
+                else:
+                    chosen = []
+                for v in chosen:
+                    vreq, vcounted = running.pop(v)
+                    vck = self.backend.checkpoint(v)
+                    self.backend.evict(v)
+                    st.preemptions += 1
+                    waiting.append([vreq, vck, vcounted])
+                if chosen:
+                    slot = self._place(req, ckpt)
+                    waiting.sort(key=lambda w: (-w[0].priority, w[0].arrival))
+            if slot < 0:
+                break
+            del waiting[next(i for i, w in enumerate(waiting) if w is head)]
+            running[slot] = (req, counted)
+            if ckpt is None:
+                st.admitted += 1
 
     def run(self, requests: list, max_wall_s: float) -> ServeStats:
         st = ServeStats()
         pending = deque(sorted(requests, key=lambda r: r.arrival))
-        queue: deque = deque()
-        running = {}          # slot -> (request, steps already counted)
+        waiting: list = []     # [request, checkpoint or None, steps counted]
+        running = {}           # slot -> (request, steps already counted)
         k = 1
         t0 = self.clock()
         while True:
             now = self.clock() - t0
-            if now >= max_wall_s or not (pending or queue or running):
+            if now >= max_wall_s or not (pending or waiting or running):
                 break
+            arrived = False
             while pending and pending[0].arrival <= now:
-                queue.append(pending.popleft())
+                waiting.append([pending.popleft(), None, 0])
                 st.arrived += 1
-            while queue:
-                slot = self.backend.try_admit(queue[0])
-                if slot < 0:
-                    break
-                running[slot] = (queue.popleft(), 0)
-                st.admitted += 1
-            st.queue_samples.append((now, len(queue), len(running)))
+                arrived = True
+            if arrived and self.preempt:
+                waiting.sort(key=lambda w: (-w[0].priority, w[0].arrival))
+            self._admit(st, waiting, running)
+            st.queue_samples.append((now, len(waiting), len(running)))
             if not running:
                 if pending:
                     self.sleep(max(0.0, min(pending[0].arrival - now, max_wall_s - now)))
-                continue
+                    continue
+                break  # nothing runs, nothing can be admitted, nothing arrives
             c0 = self.clock()
             self.backend.steps(k)
             active, nstep, _ = self.backend.table()
@@ -173,7 +243,7 @@ class Server:
             if dtc > 0:
                 k = int(max(1, min(self.max_chunk, round(k * self.chunk_target_s / dtc))))
         st.wall_s = self.clock() - t0
-        arrived_waiting = len(queue) + sum(1 for r in pending if r.arrival <= st.wall_s)
+        arrived_waiting = len(waiting) + sum(1 for r in pending if r.arrival <= st.wall_s)
         st.arrived += sum(1 for r in pending if r.arrival <= st.wall_s)
         st.queue_samples.append((st.wall_s, arrived_waiting, len(running)))
         st.unfinished = len(running)

@@ -39,3 +39,25 @@ def test_served_results_equal_alone(product_lib):
     assert max(q for _, q, _ in st.queue_samples) > 0  # some requests had to wait
     for req in reqs:
         assert bitwise_equal(be.results[req.rid], solve_alone(req)), req.rid
+
+
+def test_preempted_solves_resume_bit_for_bit(product_lib):
+    """A budget for two mid-size solves; high-priority requests arriving later
+    evict low-priority ones (checkpoint to the host, removal), which resume
+    when memory frees up.  Every result equals the request solved alone."""
+    import dataclasses
+    base = poisson_requests(6, 1e4, seed=21, side_lo=96, side_hi=128, tend_lo=0.004,
+                            tend_hi=0.006)
+    # low priority: long solves (about 250 steps) from t = 0; high priority:
+    # short ones arriving 2 ms later, while the first ones run
+    reqs = [dataclasses.replace(r, arrival=0.0, tend=0.05, priority=0) for r in base[:3]]
+    reqs += [dataclasses.replace(r, arrival=0.002, priority=3) for r in base[3:]]
+    budget = 2 * Batch.bytes_needed(make_params(128, 128)) + 4096
+    be = BatchBackend(make_params(64, 64), budget, capacity=8, keep_results=True)
+    st = Server(be, chunk_target_s=0.002, preempt=True).run(reqs, max_wall_s=120.0)
+    be.close()
+    s = st.summary()
+    assert s["completed"] == len(reqs), s
+    assert s["preemptions"] >= 1, s
+    for req in reqs:
+        assert bitwise_equal(be.results[req.rid], solve_alone(req)), req.rid

@@ -31,6 +31,7 @@ class SimBackend:
         self.capacity = capacity
         self.slots = {}
         self.admitted_order = []
+        self.resumed = []
         self.peak = 0
 
     @staticmethod
@@ -68,6 +69,25 @@ class SimBackend:
 
     def release(self, slot, req):
         del self.slots[slot]
+
+    # preemption: a checkpoint is the request and its step count
+    def checkpoint(self, slot):
+        req, n = self.slots[slot]
+        return {"req": req, "n": n, "nx": req.side, "ny": req.side}
+
+    def evict(self, slot):
+        del self.slots[slot]
+
+    def try_resume(self, ck):
+        slot = self.try_admit(ck["req"])
+        if slot >= 0:
+            self.slots[slot] = (ck["req"], ck["n"])
+            self.resumed.append(ck["req"].rid)
+        return slot
+
+    def fits_after(self, req, ck, slots):
+        freed = sum(self.slots[s][0].cells for s in slots)
+        return self.used() - freed + req.cells <= self.budget
 
 
 def test_poisson_requests_are_seeded_and_in_range():
@@ -122,3 +142,43 @@ def test_head_of_line_waits_for_memory():
     st = Server(be, clock=clk, sleep=clk.sleep).run(reqs, max_wall_s=1e3)
     assert be.admitted_order == [1, 3, 2]
     assert len(st.completed) == 3
+
+
+def test_preemption_by_priority_loses_no_work():
+    """Two low-priority solves fill the budget; a high-priority request arrives,
+    evicts the latest low-priority one, finishes first, and the evicted solve
+    resumes from its checkpoint: every solve completes with exactly its own
+    step count and the work adds up."""
+    clk = FakeClock()
+    be = SimBackend(clk, budget_cells=2 * 100 * 100, cost=1e-6)
+    reqs = [Request(1, 0.0, 100, 0.5, .5, .5, 1., 1., priority=0),
+            Request(2, 0.001, 100, 0.5, .5, .5, 1., 1., priority=0),
+            Request(3, 0.02, 100, 0.1, .5, .5, 1., 1., priority=5)]
+    st = Server(be, clock=clk, sleep=clk.sleep, preempt=True, chunk_target_s=0.01).run(
+        reqs, max_wall_s=1e3)
+    assert st.preemptions == 1 and be.resumed == [2]
+    assert be.peak <= be.budget
+    done = {rid: n for rid, _, n, _ in st.completed}
+    assert done == {r.rid: SimBackend.steps_needed(r) for r in reqs}
+    order = [rid for rid, *_ in st.completed]
+    assert order.index(3) < order.index(2)
+    assert st.cell_steps == sum(r.cells * SimBackend.steps_needed(r) for r in reqs)
+
+
+def test_no_preemption_without_priority_or_room():
+    """Equal priorities never preempt; nor does a request that would not fit
+    even after evicting every lower-priority solve."""
+    clk = FakeClock()
+    be = SimBackend(clk, budget_cells=2 * 100 * 100, cost=1e-6)
+    reqs = [Request(1, 0.0, 100, 0.3, .5, .5, 1., 1.),
+            Request(2, 0.0, 100, 0.3, .5, .5, 1., 1.),
+            Request(3, 0.01, 100, 0.1, .5, .5, 1., 1.)]
+    st = Server(be, clock=clk, sleep=clk.sleep, preempt=True).run(reqs, max_wall_s=1e3)
+    assert st.preemptions == 0 and be.admitted_order == [1, 2, 3]
+    clk = FakeClock()
+    be = SimBackend(clk, budget_cells=2 * 100 * 100, cost=1e-6)
+    reqs = [Request(1, 0.0, 100, 0.3, .5, .5, 1., 1., priority=1),
+            Request(2, 0.0, 100, 0.3, .5, .5, 1., 1., priority=0),
+            Request(3, 0.01, 150, 0.1, .5, .5, 1., 1., priority=9)]
+    st = Server(be, clock=clk, sleep=clk.sleep, preempt=True).run(reqs, max_wall_s=1e3)
+    assert st.preemptions == 0 and len(st.completed) == 2
