@@ -173,9 +173,26 @@ struct MixedStages {
 
     static __device__ __forceinline__ Flux riemann(const Consts& C, const Prim& ql, const Prim& qr) {
         // First guess (FP32).
-        const float rl = fmaxf(ql.r, C.smallr), ul = ql.u, pl = fmaxf(ql.p, rl * C.smallp);
-        const float rr = fmaxf(qr.r, C.smallr), ur = qr.u, pr = fmaxf(qr.p, rr * C.smallp);
-        const float cl = C.gamma * pl * rl, cr = C.gamma * pr * rr;
+        float rl = fmaxf(ql.r, C.smallr), pl = fmaxf(ql.p, rl * C.smallp);
+        float rr = fmaxf(qr.r, C.smallr), pr = fmaxf(qr.p, rr * C.smallp);
+        const float ul = ql.u, ur = qr.u;
+        float cl = C.gamma * pl * rl, cr = C.gamma * pr * rr;
+        // gamma p rho multiplies two small numbers: near vacuum (density near
+        // smallr, pressure near smallp) it falls below the FP32 normal range
+        // and would be flushed to zero.  The solve is covariant under scaling
+        // density and pressure by one factor a (velocities and sound speeds
+        // unchanged; rho*, p*, W and the fluxes scale by a, W^2 by a^2), so
+        // such an interface is solved with both scaled by a = 2^k, which is
+        // exact, and its flux scaled back in FP64.  Other interfaces have
+        // k = 0 and the arithmetic is untouched.
+        float a = 1.f;
+        if (!(cl >= 1e-30f && cr >= 1e-30f)) {
+            const int e = ilogbf(rl) + ilogbf(pl) + ilogbf(rr) + ilogbf(pr);
+            a = ldexpf(1.f, -e / 4);  // geometric mean of rho p on both sides near 1
+            rl *= a; pl *= a; rr *= a; pr *= a;
+            cl = C.gamma * pl * rl;
+            cr = C.gamma * pr * rr;
+        }
         const float wl0 = sqrtf(cl), wr0 = sqrtf(cr);
         const float p0 = fmaxf(((wr0 * pl + wl0 * pr) + wl0 * wr0 * (ul - ur)) / (wl0 + wr0), 0.f);
 
@@ -197,21 +214,26 @@ struct MixedStages {
             double delp = (usl - usr) * rcp64(iql + iqr);
             delp = delp > -pst ? delp : -pst;
             pst += delp;
-            if (!(fabs(delp) > 1e-6 * fabs(pst + C.smallppd))) break;
+            if (!(fabs(delp) > 1e-6 * fabs(pst + C.smallppd * a))) break;
         }
         const float ps = (float)pst;
 
         // Sampling (FP32).
         const float wr = sqrtf(cr * (1.f + C.gamma6 * (ps - pr) / pr));
         const float wl = sqrtf(cl * (1.f + C.gamma6 * (ps - pl) / pl));
-        const float ustar = 0.5f * (ul + (pl - ps) / wl + ur - (pr - ps) / wr);
+        // u* grouped as (ul + ur) + (left term - right term): a mirror pair
+        // (a reflecting wall: ur = -ul, identical pressures and W) gives
+        // u* = 0 exactly, so the wall's mass and energy fluxes vanish
+        // exactly.  The reference's order, ul + A_l + ur - A_r, leaves FP32
+        // rounding of A, which is large next to near-vacuum states.
+        const float ustar = 0.5f * ((ul + ur) + ((pl - ps) / wl - (pr - ps) / wr));
         const bool left = ustar > 0.f;
         const float sgnm = left ? 1.f : -1.f;
         const float ro = left ? rl : rr, uo = left ? ul : ur, po = left ? pl : pr;
         const float wo = left ? wl : wr;
         const float iro = 1.0f / ro;
         const float co = fmaxf(C.smallc, sqrtf(fabsf(C.gamma * po * iro)));
-        const float rstar = fmaxf(ro / (1.f + ro * (po - ps) / (wo * wo)), C.smallr);
+        const float rstar = fmaxf(ro / (1.f + ro * (po - ps) / (wo * wo)), C.smallr * a);
         const float cstar = fmaxf(C.smallc, sqrtf(fabsf(C.gamma * ps / rstar)));
         float spout = co - sgnm * uo;
         float spin = cstar - sgnm * ustar;
@@ -241,7 +263,15 @@ struct MixedStages {
         const float ekin = 0.5f * gr * (gu * gu + gv * gv);
         const float etot = gp * C.entho + ekin;
         const FluxF f{mass, mass * gu + gp, mass * gv, gu * (etot + gp)};
-        return Flux{(double)f.d, (double)f.mn, (double)f.mt, (double)f.e};
+        Flux out{(double)f.d, (double)f.mn, (double)f.mt, (double)f.e};
+        if (a != 1.f) {
+            const double ia = 1.0 / (double)a;  // a power of two: exact
+            out.d *= ia;
+            out.mn *= ia;
+            out.mt *= ia;
+            out.e *= ia;
+        }
+        return out;
     }
 
     // FP64 update with the flux difference formed in FP64 (the FP32 fluxes

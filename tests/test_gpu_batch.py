@@ -153,3 +153,25 @@ def test_checkpoint_resume_is_seamless(product_lib, precision, at):
     assert b.status(s2)["nstep"] == 13
     assert bitwise_equal(b.download(s2), want)
     b.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batch_random_states_equal_single_runs(product_lib, precision):
+    """Instances whose cells are all drawn at random (shocks everywhere,
+    near-vacuum cells; see _helpers.random_state) in one batch: each equals
+    its single-domain run bit for bit."""
+    from _helpers import random_state
+    inst = []
+    for k, (nx, ny, kind) in enumerate([(37, 29, "rough"), (64, 48, "vacuum"), (130, 24, "smooth"),
+                                         (24, 96, "vacuum"), (80, 80, "rough")]):
+        inst.append((make_params(nx, ny), random_state(nx, ny, 100 + k, kind)))
+    b = Batch(inst[0][0], capacity=8, arena_bytes=ARENA, precision=precision)
+    slots = [b.add(H, u) for H, u in inst]
+    b.steps(12)
+    for s, (H, u0) in zip(slots, inst):
+        want, t, n = alone(H, u0, 12, precision)
+        st = b.status(s)
+        assert st["nstep"] == n == 12 and st["t"] == t
+        got = b.download(s)
+        assert bitwise_equal(got, want), (H.nx, H.ny, describe_mismatch(got, want))
+    b.close()

@@ -104,3 +104,26 @@ def test_make_boundary_matches_reference_live(oracle):
             r.make_boundary(idim)
             assert bitwise_equal(u, r.get()), (bnd, idim)
         r.close()
+
+
+@ref_needed
+@pytest.mark.parametrize("kind,seed,extra", [
+    ("rough", 1, {}), ("smooth", 2, {}), ("vacuum", 3, {}),
+    ("rough", 4, {"scheme": 2}), ("vacuum", 5, {"scheme": 3, "slope_type": 0.7}),
+    ("rough", 6, {"iorder": 1, "niter_riemann": 3}),
+])
+def test_restatement_matches_reference_on_random_states(oracle, kind, seed, extra):
+    """Random states (see _helpers.random_state), 16 steps, both codes from
+    the same input: every cell and every dt bit for bit."""
+    from _helpers import random_state
+    p = oracle.make_param(37, 29, boundary=(1, 2, 3, 1) if seed % 2 else (1, 1, 1, 1), **extra)
+    u = random_state(37, 29, seed, kind)
+    r = oracle.RefState(p, 0, nxystep=5)
+    r.set(u)
+    n, dts, _ = oracle.run(p, u, 16)
+    n2, dts2, _, _, _ = r.run(16)
+    ur = r.get()
+    r.close()
+    assert np.all(np.isfinite(u))
+    assert n == n2 and bitwise_equal(dts, dts2)
+    assert bitwise_equal(u, ur), describe_mismatch(u, ur)
