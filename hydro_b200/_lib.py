@@ -21,6 +21,7 @@ HB_OK, HB_ERR_ARG, HB_ERR_CUDA, HB_ERR_NODEV, HB_ERR_NOMEM, HB_ERR_STATE, HB_ERR
 HB_PREC_FP64, HB_PREC_MIXED = 0, 1
 PRECISIONS = {"fp64": HB_PREC_FP64, "mixed": HB_PREC_MIXED}
 HB_XSWEEP_MARCH, HB_XSWEEP_CELL = 0, 1
+HB_NOALLOC_MAX_CELLS = 1 << 20  # include/hydro_b200.h
 XSWEEPS = {"march": HB_XSWEEP_MARCH, "cell": HB_XSWEEP_CELL}
 
 

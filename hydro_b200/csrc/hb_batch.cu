@@ -132,7 +132,7 @@ struct hb_batch {
 namespace {
 
 long long units_for(const hydroparam_t* H) {
-    const long long vs = (long long)(H->nx + 4) * (H->ny + 4);
+    const long long vs = ((long long)H->nx + 4) * ((long long)H->ny + 4);
     return (4 * vs + 31) / 32;  // one buffer, rounded to 256 bytes
 }
 
@@ -387,7 +387,10 @@ extern "C" long long hydro_b200_batch_arena_free(hb_batch* b) {
 }
 
 extern "C" long long hydro_b200_batch_bytes_needed(const hydroparam_t* H) {
-    return H ? 2 * units_for(H) * 256 : 0;
+    if (!H || H->nx < 3 || H->ny < 3 ||
+        ((long long)H->nx + 4) * ((long long)H->ny + 4) > (1ll << 31))
+        return 0;  // not an admissible grid
+    return 2 * units_for(H) * 256;
 }
 
 // Admit an instance: its grid (nx, ny, dx, boundary types) from H, its state
@@ -413,7 +416,7 @@ static int batch_add_impl(hb_batch* b, const hydroparam_t* H, const double* host
                           int nstepmax, double dt0) {
     if (!b || !H || !host) return fail(HB_ERR_ARG, "add: null argument"), -1;
     if (H->nx < 3 || H->ny < 3 || !(H->dx > 0.0) ||
-        (long long)(H->nx + 4) * (H->ny + 4) > (1ll << 31))
+        ((long long)H->nx + 4) * ((long long)H->ny + 4) > (1ll << 31))
         return fail(HB_ERR_ARG, "add: unsupported grid"), -1;
     if (sync_table_down(b) != HB_OK) return -1;
     int slot = -1;

@@ -102,7 +102,7 @@ extern "C" int hydro_b200_godunov_noalloc(const hydroparam_t* H, double* d_uold,
     if (H->nvar != 4 || H->nx < 3 || H->ny < 3 || H->scheme < 1 || H->scheme > 3 ||
         !(H->dx > 0.0) || H->niter_riemann < 0)
         return hb_record_error(HB_ERR_ARG, "noalloc: unsupported parameter set");
-    if ((long long)(H->nx + 4) * (H->ny + 4) > HB_NOALLOC_MAX_CELLS)
+    if (((long long)H->nx + 4) * ((long long)H->ny + 4) > HB_NOALLOC_MAX_CELLS)
         return hb_record_error(HB_ERR_ARG,
                                "noalloc: grid too large: (nx+4)*(ny+4) must be <= "
                                "HB_NOALLOC_MAX_CELLS (1048576 padded cells, 32 MiB of scratch)");

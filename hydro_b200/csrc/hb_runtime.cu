@@ -110,6 +110,8 @@ static int validate(const hydroparam_t* H) {
                          H->nvar);
     if (H->nx < 3 || H->ny < 3)
         return set_error(HB_ERR_ARG, "grid %dx%d: nx and ny must be >= 3", H->nx, H->ny);
+    if (((long long)H->nx + 4) * ((long long)H->ny + 4) > (1ll << 31))
+        return set_error(HB_ERR_ARG, "grid too large for 32-bit line indices");
     if ((H->nxt && H->nxt != H->nx + 4) || (H->nyt && H->nyt != H->ny + 4))
         return set_error(HB_ERR_ARG, "nxt/nyt (%d,%d) must be nx+4, ny+4", H->nxt, H->nyt);
     if (H->scheme < 1 || H->scheme > 3)
@@ -117,8 +119,6 @@ static int validate(const hydroparam_t* H) {
                          H->scheme);
     if (!(H->dx > 0.0)) return set_error(HB_ERR_ARG, "dx must be > 0");
     if (H->niter_riemann < 0) return set_error(HB_ERR_ARG, "niter_riemann < 0");
-    if ((long long)(H->nx + 4) * (H->ny + 4) > (1ll << 31))
-        return set_error(HB_ERR_ARG, "grid too large for 32-bit line indices");
     return HB_OK;
 }
 
