@@ -38,6 +38,8 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from hydro_b200.metrics import field_errors  # noqa: E402
+
 WORKLOADS = {
     "c1": dict(name="hydroc_4096x4096_centre_blast_fp64", nx=4096, ny=4096, testcase=0,
                run_steps=200),
@@ -284,12 +286,36 @@ def run_batched_form(device, seed=20261203, n=256, nsteps=100):
     done = int(sum(1 for s in slots if nstep[s] == nsteps))
     cells = sum(H.nx * H.ny for H, _ in mix)
     launches = b.launch_count - l0
+    # Accuracy of what was served: every 16th instance against its FP64 run.
+    worst = {"rho": 0.0, "E": 0.0}
+    for i in range(0, n, 16):
+        H, u = mix[i]
+        ref = dom_state_after(H, u, nsteps, "fp64")
+        err = field_errors(b.download(slots[i]), ref)
+        for v in worst:
+            worst[v] = max(worst[v], err[v]["l1_rel"])
     b.close()
     return {"workload": f"{n} seeded blast instances, sides 64..1024, {nsteps} steps each",
             "value": round(cells * nsteps / (ms / 1e3) / 1e6, 3), "unit": "Mcell-updates/s",
             "ms": round(ms, 3), "instances_finished": done, "cells": cells,
             "graph_launches": nsteps, "kernel_launches": launches, "tuning": tuning,
-            "precision": "mixed"}
+            "precision": "mixed",
+            "l1_rel_vs_fp64_max": {"sample": f"{len(range(0, n, 16))} of {n} instances",
+                                   **{v: float(f"{x:.3g}") for v, x in worst.items()}}}
+
+
+def solve_fp64(req):
+    """A served request solved alone in FP64 until its tend."""
+    from hydro_b200 import Batch
+    from hydro_b200.batch import blast_spec, blast_state
+    H, rho, e_bg, cell, eb = blast_spec(req.side, req.side, req.bx, req.by, req.e0, req.rho)
+    b = Batch(H, capacity=1, arena_bytes=Batch.bytes_needed(H) + 4096, precision="fp64")
+    s = b.add(H, blast_state(H, rho, e_bg, cell, eb), tend=req.tend)
+    while b.status(s)["active"]:
+        b.steps(64)
+    u = b.download(s)
+    b.close()
+    return u
 
 
 def run_serving_form(label, rate, n, side_lo, side_hi, tend_lo, tend_hi, wall_s, seed=20261204):
@@ -301,10 +327,21 @@ def run_serving_form(label, rate, n, side_lo, side_hi, tend_lo, tend_hi, wall_s,
     free, total = torch.cuda.mem_get_info()
     budget = int(0.8 * free)
     reqs = poisson_requests(n, rate, seed, side_lo, side_hi, tend_lo, tend_hi)
-    be = BatchBackend(make_params(128, 128), budget, capacity=4096)
+    # Accuracy of what was served: the first few small requests are kept and
+    # compared with their FP64 solves.
+    sample = set([r.rid for r in reqs if r.side <= 256][:6])
+    be = BatchBackend(make_params(128, 128), budget, capacity=4096, keep_results=sample)
     st = Server(be).run(reqs, max_wall_s=wall_s)
     be.close()
     out = st.summary()
+    worst = {"rho": 0.0, "E": 0.0}
+    by_id = {r.rid: r for r in reqs}
+    for rid, u in be.results.items():
+        err = field_errors(u, solve_fp64(by_id[rid]))
+        for v in worst:
+            worst[v] = max(worst[v], err[v]["l1_rel"])
+    out["l1_rel_vs_fp64_max"] = {"sample": f"{len(be.results)} completed requests of side <= 256",
+                                 **{v: float(f"{x:.3g}") for v, x in worst.items()}}
     out.update({"label": label, "lambda_per_s": rate, "requests_offered": n,
                 "sides": [side_lo, side_hi], "tend": [tend_lo, tend_hi],
                 "hbm_budget_gb": round(budget / 1e9, 1), "wall_limit_s": wall_s,
@@ -460,7 +497,6 @@ def main():
     # against the FP64 state.
     forms = {}
     if not args.no_mixed:
-        from hydro_b200.metrics import field_errors
         ref_state = dom_state_after(H, u0, K, "fp64")
         dm = Domain(H, precision="mixed")
         dm.upload(u0)

@@ -73,7 +73,9 @@ class BatchBackend:
     """GPU backend: one hb_batch whose arena is the HBM budget."""
 
     def __init__(self, H, budget_bytes: int, capacity: int = 1024, precision: str = "mixed",
-                 keep_results: bool = False):
+                 keep_results=False):
+        """keep_results: True to keep every finished state (host memory), or a
+        set of request ids to keep only those."""
         self.batch = Batch(H, capacity, budget_bytes, precision=precision)
         self.capacity = capacity
         self.keep_results = keep_results
@@ -109,7 +111,8 @@ class BatchBackend:
         self.batch.remove(slot)
 
     def release(self, slot: int, req: Request) -> None:
-        if self.keep_results:
+        keep = self.keep_results
+        if keep is True or (keep and req.rid in keep):
             self.results[req.rid] = self.batch.download(slot)
         self.batch.remove(slot)
 
