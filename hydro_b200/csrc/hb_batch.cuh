@@ -52,6 +52,12 @@ constexpr int kBatchCourSlots = 16; // Courant accumulator slots per instance
 // the kernel latency-bound; 14 is 5% faster per step in both precisions, 16
 // slower again.
 constexpr int kBatchXMinBlocks = 14;
+// The same for the mixed-precision y-item kernel (marching, prefetching):
+// uncapped it takes 147 registers (6 CTAs per SM); 7 CTAs is 3% faster per
+// batched step, 8 less so.
+constexpr int kBatchYMixedMinBlocks = 7;
+// The FP64 y-item kernel takes the plain FP64 march's cap (kFp64MarchMinBlocks,
+// 64 registers): 134 registers uncapped, 15% slower per batched step.
 constexpr int kXItemWindows = 8;    // cell windows per x item (4 per warp)
 
 struct BatchLaunch {

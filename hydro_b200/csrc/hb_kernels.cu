@@ -235,7 +235,7 @@ cudaError_t launch_clock_end(DevClock* c, cudaStream_t s) {
 
 // ---------------------------------------------------------------- batches
 template <bool UNIT, int DIR>
-__global__ void __launch_bounds__(kBatchThreads, DIR == 1 ? kBatchXMinBlocks : 1)
+__global__ void __launch_bounds__(kBatchThreads, DIR == 1 ? kBatchXMinBlocks : kFp64MarchMinBlocks)
 batch_sweep_kernel(const BatchLaunch L, const Phys P) {
     batch_sweep_body<ExactStages<UNIT>, DIR>(L, P);
 }

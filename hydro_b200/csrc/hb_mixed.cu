@@ -47,7 +47,7 @@ int sweep_mixed_blocks_per_sm(int dir) {
 }
 
 template <int DIR>
-__global__ void __launch_bounds__(kBatchThreads, DIR == 1 ? kBatchXMinBlocks : 1)
+__global__ void __launch_bounds__(kBatchThreads, DIR == 1 ? kBatchXMinBlocks : kBatchYMixedMinBlocks)
 batch_sweep_mixed_kernel(const BatchLaunch L, const Phys P) {
     batch_sweep_body<MixedStages, DIR>(L, P);
 }
