@@ -211,14 +211,15 @@ int hydro_b200_domain_courant(hb_domain *d, double *cournox, double *cournoy); /
  * on the domain's stream. */
 int hydro_b200_domain_sweep(hb_domain *d, int stage, int idim, double dt, int fuse_courant);
 long long hydro_b200_domain_halo_count(hb_domain *d, int idim);
+int hydro_b200_domain_halo_pack(hb_domain *d, int stage, int idim, int side, double *dst);
+int hydro_b200_domain_halo_unpack(hb_domain *d, int idim, int side, const double *src);
+
 /* VTK payload of one variable (0..3 = rho, rho u, rho v, E): the interior in
  * row order as floats (C's (float) cast), base64-encoded as vtkfile.c:262-280
  * does, written to host memory; hydro_b200_vtk_base64_len(nx, ny) bytes (no
  * terminator; the 8-character length header is not included). */
 long long hydro_b200_vtk_base64_len(int nx, int ny);
 int hydro_b200_domain_vtk_base64(hb_domain *d, int var, char *host_out, long long cap);
-int hydro_b200_domain_halo_pack(hb_domain *d, int stage, int idim, int side, double *dst);
-int hydro_b200_domain_halo_unpack(hb_domain *d, int idim, int side, const double *src);
 /* Launch-only driver (asynchronous; same semantics as hydro_b200_run). */
 int hydro_b200_domain_set_clock(hb_domain *d, double t, int nstep, double dt);
 int hydro_b200_domain_launch_steps(hb_domain *d, int nsteps, int nstepmax, double tend);
@@ -254,9 +255,10 @@ long long hydro_b200_domain_launch_count(hb_domain *d);
 /* ------------------------------------------------------------------------
  * Batches: many independent runs of different grid sizes advanced together.
  * One global step advances every active instance by one time step of its own
- * (its own dt, main.c:344-408 semantics per instance) with two persistent
- * launches that pull work items of all instances from a queue; each step is
- * replayed as a CUDA graph.  Instance states live in one device arena.
+ * (its own dt, main.c:344-408 semantics per instance) with persistent
+ * launches (x items and y items of each sweep phase) that pull work items of
+ * all instances from a queue; each step is replayed as a CUDA graph.
+ * Instance states live in one device arena.
  * ------------------------------------------------------------------------ */
 typedef struct hb_batch hb_batch;
 /* H supplies the constants shared by every instance (gamma, smallr, smallc,
