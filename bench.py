@@ -217,22 +217,14 @@ def run_vtk_form(H, u):
             from oracle import oracle as O
             if not O.ref_available():
                 raise RuntimeError("reference not compiled")
-            ref = O.RefState(O.make_param(H.nx, H.ny), 0)
             os.chdir(dirs[1])
-            devnull = os.open(os.devnull, os.O_WRONLY)
-            saved = os.dup(1)
-            try:
-                sys.stdout.flush()
-                os.dup2(devnull, 1)  # vtkfile.c prints the decomposition once
+            with quiet_stdout():  # the reference prints its set-up and decomposition
+                ref = O.RefState(O.make_param(H.nx, H.ny), 0)
                 t0 = time.perf_counter()
                 ref.set(run.sync_to_host())
                 ref.vtkfile(1)
                 ref_ms = (time.perf_counter() - t0) * 1e3
-            finally:
-                os.dup2(saved, 1)
-                os.close(saved)
-                os.close(devnull)
-            ref.close()
+                ref.close()
             names = [os.path.relpath(os.path.join(dp, f), dirs[0])
                      for dp, _, fs in os.walk(dirs[0]) for f in fs]
             out["files_identical"] = all(filecmp.cmp(os.path.join(dirs[0], n),
@@ -349,6 +341,24 @@ def run_serving_form(label, rate, n, side_lo, side_hi, tend_lo, tend_hi, wall_s,
     return out
 
 
+class quiet_stdout:
+    """Route file descriptor 1 to /dev/null (the reference's C code prints
+    set-up messages), so that the bench's stdout is its JSON line alone."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.devnull = os.open(os.devnull, os.O_WRONLY)
+        self.saved = os.dup(1)
+        os.dup2(self.devnull, 1)
+        return self
+
+    def __exit__(self, *exc):
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        os.close(self.devnull)
+        return False
+
+
 def cpu_reference_sample(wl, budget_s, max_steps, warm=1):
     """The reference's own C99/OpenMP code (oracle/_ref) on the host cores,
     falling back to the C restatement (oracle/_build) where the reference was
@@ -360,13 +370,14 @@ def cpu_reference_sample(wl, budget_s, max_steps, warm=1):
     O.oracle_lib().orc_set_threads(cores)
     if O.ref_available():
         kind = "reference"
-        r = O.RefState(p, wl["testcase"], nxystep=256)
-        t0 = time.perf_counter()
-        r.run(warm)
-        tw = time.perf_counter() - t0
-        nrun = max(1, min(max_steps, int(budget_s / max(tw / max(warm, 1), 1e-6))))
-        n, dts, _, mcs_avg, el = r.run(warm + nrun)
-        r.close()
+        with quiet_stdout():
+            r = O.RefState(p, wl["testcase"], nxystep=256)
+            t0 = time.perf_counter()
+            r.run(warm)
+            tw = time.perf_counter() - t0
+            nrun = max(1, min(max_steps, int(budget_s / max(tw / max(warm, 1), 1e-6))))
+            n, dts, _, mcs_avg, el = r.run(warm + nrun)
+            r.close()
         desc = (f"reference C99/OpenMP (oracle/_ref, gcc -O3 -fopenmp -mavx2) on "
                 f"{wl['nx']}x{wl['ny']}: steps {warm}..{warm + n - 1} after {warm} warm-up "
                 f"step(s), {cores} OpenMP threads")
