@@ -13,7 +13,8 @@ line cannot be admitted, running solves of lower priority are checkpointed to
 host memory and removed (the reference's Continue.dump restart files,
 CPP/Domain_Prot.cpp:284-411, held in memory) until it fits; they wait with
 their checkpoint and resume bit for bit when memory frees up.  Waiting solves
-are admitted by priority, then arrival.
+are admitted by priority, then arrival.  A request larger than the whole
+budget is rejected at arrival instead of blocking the line.
 
 The loop talks to a backend (``BatchBackend`` for the GPU); the bookkeeping
 is independent of it, so it is tested on the CPU with a simulated backend.
@@ -77,6 +78,7 @@ class BatchBackend:
         """keep_results: True to keep every finished state (host memory), or a
         set of request ids to keep only those."""
         self.batch = Batch(H, capacity, budget_bytes, precision=precision)
+        self.budget = budget_bytes
         self.capacity = capacity
         self.keep_results = keep_results
         self.results = {}
@@ -91,6 +93,10 @@ class BatchBackend:
 
     def table(self):
         return self.batch.table()
+
+    def can_ever_fit(self, req: Request) -> bool:
+        """Whether the request fits the arena at all (an empty one)."""
+        return Batch.bytes_needed(make_params(req.side, req.side)) <= self.budget
 
     def checkpoint(self, slot: int) -> dict:
         return self.batch.checkpoint(slot)
@@ -131,6 +137,7 @@ class ServeStats:
     chunks: int = 0
     unfinished: int = 0
     preemptions: int = 0
+    rejected: int = 0
 
     def summary(self) -> dict:
         lat = np.array([c[1] for c in self.completed]) if self.completed else np.zeros(0)
@@ -147,6 +154,7 @@ class ServeStats:
             "running_end": self.unfinished,
             "chunks": self.chunks,
             "preemptions": self.preemptions,
+            "rejected": self.rejected,
         }
 
 
@@ -215,8 +223,12 @@ class Server:
                 break
             arrived = False
             while pending and pending[0].arrival <= now:
-                waiting.append([pending.popleft(), None, 0])
+                req = pending.popleft()
                 st.arrived += 1
+                if not self.backend.can_ever_fit(req):
+                    st.rejected += 1  # larger than the whole budget: it would block the line
+                    continue
+                waiting.append([req, None, 0])
                 arrived = True
             if arrived and self.preempt:
                 waiting.sort(key=lambda w: (-w[0].priority, w[0].arrival))

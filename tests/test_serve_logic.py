@@ -85,6 +85,9 @@ class SimBackend:
             self.resumed.append(ck["req"].rid)
         return slot
 
+    def can_ever_fit(self, req):
+        return req.cells <= self.budget
+
     def fits_after(self, req, ck, slots):
         freed = sum(self.slots[s][0].cells for s in slots)
         return self.used() - freed + req.cells <= self.budget
@@ -182,3 +185,13 @@ def test_no_preemption_without_priority_or_room():
             Request(3, 0.01, 150, 0.1, .5, .5, 1., 1., priority=9)]
     st = Server(be, clock=clk, sleep=clk.sleep, preempt=True).run(reqs, max_wall_s=1e3)
     assert st.preemptions == 0 and len(st.completed) == 2
+
+
+def test_request_larger_than_the_budget_is_rejected_not_blocking():
+    clk = FakeClock()
+    be = SimBackend(clk, budget_cells=100 * 100, cost=1e-6)
+    reqs = [Request(1, 0.0, 200, 0.05, .5, .5, 1., 1.),   # 4x the budget
+            Request(2, 0.001, 64, 0.05, .5, .5, 1., 1.)]
+    st = Server(be, clock=clk, sleep=clk.sleep).run(reqs, max_wall_s=1e3)
+    assert st.rejected == 1 and [c[0] for c in st.completed] == [2]
+    assert st.summary()["rejected"] == 1
