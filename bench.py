@@ -394,6 +394,74 @@ def cpu_reference_sample(wl, budget_s, max_steps, warm=1):
             "sample": desc, "steps": n, "seconds": round(el, 3)}
 
 
+NML_TEMPLATE = """&RUN
+tend=1e9
+nstepmax={nsteps}
+noutput=0
+/
+&MESH
+nx={nx}
+ny={ny}
+nxystep={nxystep}
+dx={dx}
+boundary_left=1
+boundary_right=1
+boundary_down=1
+boundary_up=1
+testcase={tc}
+/
+&HYDRO
+courant_factor=0.8
+niter_riemann=10
+/
+"""
+
+
+def reference_binary_runs():
+    """The reference application itself (oracle/_ref/hydro, main.c) on the host
+    cores with OMP_NUM_THREADS = nproc and OMP_PROC_BIND = close: its own
+    "Average MC/s" line (main.c:510-513, which leaves out steps <= 5) for the
+    250x125 corner case (100 steps), the 4096^2 centred blast and a 6000^2
+    centred blast as in the reference's 6000^2 input (dx 0.05), 12 steps each."""
+    import re
+    import shutil
+    import subprocess
+    import tempfile
+    exe = os.path.join(ROOT, "oracle", "_ref", "hydro")
+    if not os.path.exists(exe):
+        return None
+    cpu_model = ""
+    try:
+        with open("/proc/cpuinfo") as f:
+            cpu_model = next((l.split(":", 1)[1].strip() for l in f if l.startswith("model name")),
+                             "")
+    except OSError:
+        pass
+    nproc = os.cpu_count() or 1
+    env = dict(os.environ, OMP_NUM_THREADS=str(nproc), OMP_PROC_BIND="close")
+    cases = [("250x125 corner blast, 100 steps", 250, 125, 125, 0.004, 1, 100),
+             ("4096x4096 centred blast, 12 steps", 4096, 4096, 256, 1.0 / 4096, 0, 12),
+             ("6000x6000 centred blast (dx 0.05), 12 steps", 6000, 6000, 1024, 0.05, 0, 12)]
+    runs = []
+    d = tempfile.mkdtemp(prefix="hb_ref_")
+    try:
+        for label, nx, ny, nxystep, dx, tc, nsteps in cases:
+            nml = os.path.join(d, "in.nml")
+            with open(nml, "w") as f:
+                f.write(NML_TEMPLATE.format(nsteps=nsteps, nx=nx, ny=ny, nxystep=nxystep,
+                                            dx=repr(dx), tc=tc))
+            r = subprocess.run([exe, "-i", nml], cwd=d, env=env, capture_output=True,
+                               text=True, timeout=600)
+            m = re.search(r"Average MC/s:\s*([0-9.eE+-]+)", r.stdout)
+            runs.append({"case": label, "average_mcs": float(m.group(1)) if m else None,
+                         "rc": r.returncode})
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+    return {"binary": "oracle/_ref/hydro (the reference application, gcc -O3 -fopenmp -mavx2)",
+            "cpu_model": cpu_model, "nproc": nproc,
+            "env": f"OMP_NUM_THREADS={nproc} OMP_PROC_BIND=close", "runs": runs}
+
+
 def run_reference_arm(args, wl):
     world, rank, local, pg = dist_setup(False)
     if rank != 0:
@@ -576,6 +644,7 @@ def main():
         budget = float(os.environ.get("HYDRO_BENCH_CPU_BUDGET_S", "20"))
         cpu = cpu_reference_sample(wl, budget, 50, warm=1)
         cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        cpu["reference_application"] = reference_binary_runs()
 
     if pg is not None:
         barrier(pg, device)
