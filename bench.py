@@ -70,6 +70,23 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
+def ncu_fp64_pipe():
+    """FP64-pipe utilisation of the two FP64 sweep kernels from the committed
+    ncu summary (percent of peak, x and y sweep), or None."""
+    import re
+    p = os.path.join(ROOT, "profiles", "sweep_fp64_2048.md")
+    try:
+        for line in open(p):
+            m = re.match(r"\|\s*FP64 pipe \(%\)\s*\|\s*([0-9.]+)\s*\|\s*([0-9.]+)\s*\|", line)
+            if m:
+                return {"x_sweep": float(m.group(1)), "y_sweep": float(m.group(2)),
+                        "unit": "% of FP64 pipe peak (ncu, 2048² capture)",
+                        "source": "profiles/sweep_fp64_2048.md"}
+    except OSError:
+        pass
+    return None
+
+
 def ncu_traffic_per_launch():
     """DRAM bytes per sweep launch from the committed ncu summary (if any)."""
     p = os.path.join(ROOT, "profiles", "sweep_fp64_4096_traffic.txt")
@@ -668,6 +685,7 @@ def main():
                      "traffic": traffic,
                      "kernel": "xcell_kernel<1> (x sweep) and sweep_kernel<2,1> (y sweep)",
                      "alg_bytes_per_launch": alg_bytes, "launch_ms": round(sweep_ms, 4),
+                     "fp64_pipe": ncu_fp64_pipe(),
                      "peak_kind": peak_kind},
         "gpu_launches": gpu_launches,
         "clocks": clocks,
