@@ -98,3 +98,43 @@ def test_split_equals_single_grid_mixed(product_lib):
     assert run.dts == dts and run.t == t
     for s in run.subs:
         s.close()
+
+
+def test_nccl_driver_single_rank(product_lib, tmp_path):
+    """The torch.distributed driver on the GPU with NCCL, one rank: the dt
+    all-reduce runs on the subdomain's stream and the run equals the
+    single-grid run bit for bit.  (Halo exchanges between ranks need two GPUs;
+    their host logic is covered by the gloo tests.)"""
+    import json
+    import os
+    import subprocess
+    import sys
+    from test_multiproc import ROOT, free_port
+    code = r"""
+import json, sys
+sys.path.insert(0, sys.argv[1])
+import numpy as np, torch, torch.distributed as dist
+from hydro_b200 import Domain, init_state, make_params
+from hydro_b200.split import DistComm, GpuSubdomain, SplitRun, decompose, local_params, scatter_state
+dist.init_process_group("nccl", init_method="env://", device_id=torch.device("cuda:0"))
+Hg = make_params(200, 120, testcase=0)
+u0 = init_state(Hg)
+box = decompose(Hg.nx, Hg.ny, 1)[0]
+sub = GpuSubdomain(local_params(Hg, box, 0, 1), box, 0, "cuda:0")
+sub.upload(scatter_state(u0, box))
+run = SplitRun(Hg, [sub], DistComm())
+run.run(24)
+got = sub.download()
+sub.close()
+d = Domain(Hg); d.upload(u0); d.set_clock(); d.launch_steps(24); want = d.download(); t = d.get_clock()[0]; d.close()
+print(json.dumps({"equal": bool(np.array_equal(got.view(np.uint64), want.view(np.uint64))),
+                  "t_equal": run.t == t}))
+dist.destroy_process_group()
+"""
+    env = dict(os.environ, RANK="0", LOCAL_RANK="0", WORLD_SIZE="1", MASTER_ADDR="127.0.0.1",
+               MASTER_PORT=str(free_port()), NCCL_NVLS_ENABLE="0")
+    r = subprocess.run([sys.executable, "-c", code, ROOT], env=env, capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stderr[-3000:]
+    rec = json.loads(r.stdout.strip().splitlines()[-1])
+    assert rec == {"equal": True, "t_equal": True}, rec
