@@ -176,7 +176,9 @@ int build_lists(hb_batch* b) {
         for (int l0 = 0; l0 < I.nx; l0 += hb::kBatchThreads)
             for (int k0 = 2; k0 < I.ny + 2; k0 += b->tune.seg)
                 L[yl][1].push_back(WorkItem{s, 2, l0, k0});
-        const int nwin = (I.nx + 2 + hb::kCellWarpOut - 1) / hb::kCellWarpOut;
+        // x windows of the stage set's width (two cells per lane in mixed precision)
+        const int wout = b->precision == HB_PREC_MIXED ? hb::kCellWarpOut2 : hb::kCellWarpOut;
+        const int nwin = (I.nx + 2 + wout - 1) / wout;
         for (int l = 0; l < I.ny; l++)
             for (int w0 = 0; w0 < nwin; w0 += hb::kXItemWindows)
                 L[xl][0].push_back(WorkItem{s, 1, l, w0});

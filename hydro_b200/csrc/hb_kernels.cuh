@@ -57,11 +57,17 @@ constexpr int kCellThreads = 64;
 // caps).  The FP64 kernels are latency-bound: more resident warps beat the
 // few register spills the caps cause (measured at 4096^2: marching y sweep
 // 1.66 -> 1.49 ms, cell-per-lane x sweep 1.63 -> 1.56 ms).  The mixed marching
-// sweep keeps its registers for the next-cell prefetch and is not capped.
+// sweep keeps its registers for the next-cell prefetch and is not capped; the
+// mixed x sweep (two cells per lane) runs best at 12 CTAs per SM (80
+// registers): 0.419 ms at 4096^2, against 0.477 ms one cell per lane.
 constexpr int kFp64MarchMinBlocks = 16;
 constexpr int kFp64CellMinBlocks = 18;
-constexpr int kMixedCellMinBlocks = 18;
-constexpr int kCellWarpOut = 28;  // outputs per warp of the cell-per-lane x sweep
+constexpr int kMixedCellMinBlocks = 12;
+constexpr int kCellWarpOut = 28;   // outputs per warp of the cell-per-lane x sweep
+constexpr int kCellWarpOut2 = 60;  // the same with two cells per lane
+// Outputs per warp of the x sweep window of a stage set.
+template <class S>
+constexpr int window_out() { return S::cells_per_lane == 2 ? kCellWarpOut2 : kCellWarpOut; }
 cudaError_t launch_xcell(const SweepArgs& a, const Phys& P, cudaStream_t s);
 cudaError_t launch_xcell_mixed(const SweepArgs& a, const Phys& P, cudaStream_t s);
 // The mixed-precision sweep (hb_mixed.cu).

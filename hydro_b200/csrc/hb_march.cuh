@@ -300,7 +300,7 @@ __device__ __forceinline__ F flux_up(const F& f) {
 // Accumulates the fused Courant maxima of its outputs into cx, cy.  The
 // caller guarantees the warp is converged and `row` < a.nlines.
 template <class S>
-__device__ __forceinline__ void xcell_window(const SweepArgs& a, const typename S::Consts& C,
+__device__ __forceinline__ void xcell_window_1(const SweepArgs& a, const typename S::Consts& C,
                                              int row, int win, double dtdx, double& cx,
                                              double& cy) {
     using Prim = typename S::Prim;
@@ -335,6 +335,80 @@ __device__ __forceinline__ void xcell_window(const SweepArgs& a, const typename 
             cy = cy > ct ? cy : ct;
         }
     }
+}
+
+// The same with two cells per lane: lane l holds cells ka = c - 2 + 2l and
+// kb = ka + 1 of a 64-cell window, c = 60 * win, and lanes 1..30 produce the
+// outputs [c, c + 60) (15 sectors).  The window's halo costs 4 of 64 cells
+// instead of 4 of 32, and each shuffle of primitives, traces or fluxes serves
+// two cells.  Every cell gets the same stage calls on the same inputs as in
+// xcell_window_1.
+template <class S>
+__device__ __forceinline__ void xcell_window_2(const SweepArgs& a, const typename S::Consts& C,
+                                               int row, int win, double dtdx, double& cx,
+                                               double& cy) {
+    using Prim = typename S::Prim;
+    using Flux = typename S::Flux;
+    using Real = typename S::Real;
+    const int lane = threadIdx.x & 31;
+    const int c = win * kCellWarpOut2;               // first output cell of the warp
+    if (c >= a.n - 2) return;                        // warp-uniform
+    const int ka = c - 2 + 2 * lane, kb = ka + 1;    // this lane's two cells
+    const LineGeom<1> g(a, row);
+    const typename S::TraceK K = S::trace_constants(C, dtdx);
+    const Cons ua = (ka >= 0 && ka < a.n) ? load_cell<1>(a, g, ka) : Cons{1.0, 0.0, 0.0, 1.0};
+    const Cons ub = (kb >= 0 && kb < a.n) ? load_cell<1>(a, g, kb) : Cons{1.0, 0.0, 0.0, 1.0};
+    Prim qa, qb;
+    Real ca, cb;
+    S::prim(C, ua, qa, ca);
+    S::prim(C, ub, qb, cb);
+    const Prim qm = prim_up(qb), qp = prim_down(qa);  // cells ka - 1, kb + 1
+    Prim dqa = S::zero_prim(), dqb = S::zero_prim();
+    if (S::second_order(C)) {
+        S::slope4(C, qm, qa, qb, dqa);
+        S::slope4(C, qa, qb, qp, dqb);
+    }
+    Prim xma, xpa, xmb, xpb;
+    S::trace(K, qa, dqa, ca, xma, xpa);
+    S::trace(K, qb, dqb, cb, xmb, xpb);
+    const Flux fab = S::riemann(C, xma, xpb);         // interface (ka | kb)
+    const Prim xpn = prim_down(xpa);                  // qxp of kb + 1
+    const Flux fbn = S::riemann(C, xmb, xpn);         // interface (kb | kb + 1)
+    const Flux fpa = flux_up(fbn);                    // interface (ka - 1 | ka)
+    if (lane >= 1 && lane <= 30) {
+        if (ka >= 2 && ka < a.n - 2) {
+            const Cons o = S::update(ua, fpa, fab, dtdx);
+            store_cell<1>(a, g, ka, o);
+            if (a.courant) {
+                double cn, ct;
+                S::courant(C, o, cn, ct);
+                cx = cx > cn ? cx : cn;
+                cy = cy > ct ? cy : ct;
+            }
+        }
+        if (kb >= 2 && kb < a.n - 2) {
+            const Cons o = S::update(ub, fab, fbn, dtdx);
+            store_cell<1>(a, g, kb, o);
+            if (a.courant) {
+                double cn, ct;
+                S::courant(C, o, cn, ct);
+                cx = cx > cn ? cx : cn;
+                cy = cy > ct ? cy : ct;
+            }
+        }
+    }
+}
+
+// The x-sweep window of a stage set (S::cells_per_lane); its outputs per
+// warp are window_out<S>().
+template <class S>
+__device__ __forceinline__ void xcell_window(const SweepArgs& a, const typename S::Consts& C,
+                                             int row, int win, double dtdx, double& cx,
+                                             double& cy) {
+    if constexpr (S::cells_per_lane == 2)
+        xcell_window_2<S>(a, C, row, win, dtdx, cx, cy);
+    else
+        xcell_window_1<S>(a, C, row, win, dtdx, cx, cy);
 }
 
 // Grid: x = rows, y = ceil(windows / warps per CTA).

@@ -20,7 +20,7 @@ xcell_mixed_kernel(const SweepArgs a, const Phys P) {
 }
 
 cudaError_t launch_xcell_mixed(const SweepArgs& a, const Phys& P, cudaStream_t s) {
-    const int nwin = (a.n - 2 + kCellWarpOut - 1) / kCellWarpOut;
+    const int nwin = (a.n - 2 + window_out<MixedStages>() - 1) / window_out<MixedStages>();
     const int wpc = kCellThreads / 32;
     dim3 grid(a.nlines, (nwin + wpc - 1) / wpc);
     xcell_mixed_kernel<<<grid, kCellThreads, 0, s>>>(a, P);
@@ -47,7 +47,7 @@ int sweep_mixed_blocks_per_sm(int dir) {
 }
 
 template <int DIR>
-__global__ void __launch_bounds__(kBatchThreads, DIR == 1 ? kBatchXMinBlocks : kBatchYMixedMinBlocks)
+__global__ void __launch_bounds__(kBatchThreads, DIR == 1 ? kBatchXMixedMinBlocks : kBatchYMixedMinBlocks)
 batch_sweep_mixed_kernel(const BatchLaunch L, const Phys P) {
     batch_sweep_body<MixedStages, DIR>(L, P);
 }

@@ -287,6 +287,7 @@ struct ExactStages {
     using Real = double;
     using TraceK = hb::TraceK;
     static constexpr bool prefetch = false;
+    static constexpr int cells_per_lane = 1;  // x sweep window (hb_march.cuh)
     static __device__ __forceinline__ Consts consts(const Phys& P) { return P; }
     static __device__ __forceinline__ Prim zero_prim() { return Prim{0.0, 0.0, 0.0, 0.0}; }
     static __device__ __forceinline__ Flux zero_flux() { return Flux{0.0, 0.0, 0.0, 0.0}; }

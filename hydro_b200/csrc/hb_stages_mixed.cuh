@@ -68,6 +68,7 @@ struct MixedStages {
     using Real = float;
     using TraceK = TraceKF;
     static constexpr bool prefetch = true;
+    static constexpr int cells_per_lane = 2;  // x sweep window (hb_march.cuh)
 
     static __device__ __forceinline__ Consts consts(const Phys& P) {
         Consts C;
