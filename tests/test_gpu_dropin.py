@@ -14,42 +14,57 @@ import pytest
 pytestmark = pytest.mark.gpu
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 REF = os.path.join(ROOT, "oracle", "_ref")
-NML = """&RUN
+NML_TEMPLATE = """&RUN
 tend=200
 nstepmax=60
 noutput=20
 /
 &MESH
-nx=250
-ny=125
-nxystep=125
-dx=0.004
-boundary_left=1
-boundary_right=1
-boundary_down=1
-boundary_up=1
-testcase=1
+nx={nx}
+ny={ny}
+nxystep={nxystep}
+dx={dx}
+boundary_left={b[0]}
+boundary_right={b[1]}
+boundary_down={b[2]}
+boundary_up={b[3]}
+testcase={tc}
 /
 &HYDRO
-courant_factor=0.8
-niter_riemann=10
+courant_factor={cf}
+niter_riemann={niter}
+scheme={scheme}
+iorder={iorder}
+slope_type={slope}
 /
 """
+# The 250x125 corner case of the bench configs, and two others that reach the
+# absorbing / periodic walls, the other schemes, first order and slope_type != 1.
+NMLS = {
+    "corner_250x125": dict(nx=250, ny=125, nxystep=125, dx=0.004, b=(1, 1, 1, 1), tc=1, cf=0.8,
+                           niter=10, scheme="muscl", iorder=2, slope=1.0),
+    "sod_absorb_plmde": dict(nx=180, ny=96, nxystep=32, dx=0.01, b=(2, 2, 1, 2), tc=2, cf=0.7,
+                             niter=10, scheme="plmde", iorder=2, slope=1.5),
+    "centre_periodic_collela": dict(nx=128, ny=160, nxystep=64, dx=0.0078125, b=(3, 3, 3, 3),
+                                    tc=0, cf=0.5, niter=5, scheme="collela", iorder=1, slope=1.0),
+}
+NML = NML_TEMPLATE.format(**NMLS["corner_250x125"])
 
 
 # hydro_dropin: the reference's own vtkfile.c reads the host array, which the
 # library copies back after every step (HYDRO_B200_SYNC=1).
 # hydro_dropin_vtk: the library's vtkfile writes from the device state; the
 # host array is never updated during the run.
+@pytest.mark.parametrize("nml", sorted(NMLS))
 @pytest.mark.parametrize("name,sync", [("hydro_dropin", "1"), ("hydro_dropin_vtk", "0")])
-def test_reference_driver_runs_on_the_gpu_path(tmp_path, product_lib, name, sync):
+def test_reference_driver_runs_on_the_gpu_path(tmp_path, product_lib, name, sync, nml):
     if not (os.path.exists(os.path.join(REF, name)) and os.path.exists(os.path.join(REF, "hydro"))):
         pytest.skip("reference application not compiled here")
     outs = {}
     for exe, env_sync in (("hydro", "0"), (name, sync)):
         d = tmp_path / exe
         d.mkdir()
-        (d / "in.nml").write_text(NML)
+        (d / "in.nml").write_text(NML_TEMPLATE.format(**NMLS[nml]))
         env = dict(os.environ, HYDRO_B200_SYNC=env_sync, OMP_NUM_THREADS="4")
         r = subprocess.run([os.path.join(REF, exe), "-i", "in.nml"], cwd=d, env=env,
                            capture_output=True, text=True, timeout=300)
