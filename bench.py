@@ -327,22 +327,37 @@ def solve_fp64(req):
     return u
 
 
-def run_serving_form(label, rate, n, side_lo, side_hi, tend_lo, tend_hi, wall_s, seed=20261204):
+def run_serving_form(label, rate, n, side_lo, side_hi, tend_lo, tend_hi, wall_s, seed=20261204,
+                     budget_bytes=None, priority_every=0):
     """The serving loop (continuous batching) on a Poisson request stream;
-    arena = 80% of the free HBM; time-bounded."""
+    arena = 80% of the free HBM unless budget_bytes is given; time-bounded.
+    With priority_every = k, every k-th request has priority 1 (the others 0)
+    and the server preempts: latencies are also reported per class."""
+    import dataclasses
     import torch
     from hydro_b200 import make_params
     from hydro_b200.serve import BatchBackend, Server, poisson_requests
     free, total = torch.cuda.mem_get_info()
-    budget = int(0.8 * free)
+    budget = int(0.8 * free) if budget_bytes is None else int(budget_bytes)
     reqs = poisson_requests(n, rate, seed, side_lo, side_hi, tend_lo, tend_hi)
+    if priority_every:
+        reqs = [dataclasses.replace(r, priority=1 if r.rid % priority_every == 0 else 0)
+                for r in reqs]
     # Accuracy of what was served: the first few small requests are kept and
     # compared with their FP64 solves.
     sample = set([r.rid for r in reqs if r.side <= 256][:6])
     be = BatchBackend(make_params(128, 128), budget, capacity=4096, keep_results=sample)
-    st = Server(be).run(reqs, max_wall_s=wall_s)
+    st = Server(be, preempt=bool(priority_every)).run(reqs, max_wall_s=wall_s)
     be.close()
     out = st.summary()
+    if priority_every:
+        prio = {r.rid: r.priority for r in reqs}
+        for cls in (1, 0):
+            lat = np.array([c[1] for c in st.completed if prio[c[0]] == cls])
+            out[f"priority_{cls}"] = {
+                "completed": int(lat.size),
+                "p50_s": round(float(np.percentile(lat, 50)), 4) if lat.size else None,
+                "p99_s": round(float(np.percentile(lat, 99)), 4) if lat.size else None}
     worst = {"rho": 0.0, "E": 0.0}
     by_id = {r.rid: r for r in reqs}
     for rid, u in be.results.items():
@@ -630,6 +645,11 @@ def main():
         forms["serving_subsaturating"] = run_serving_form(
             "sub-saturating stream (labelled): lambda 20/s, sides 128..512, tend 0.01..0.03",
             20.0, 400, 128, 512, 0.01, 0.03, args.serving_wall)
+        forms["serving_priority"] = run_serving_form(
+            "priority mix (labelled): lambda 15/s, sides 128..768, tend 0.01..0.03, every 4th "
+            "request priority 1 with preemption, 128 MB arena (memory-bound on purpose)",
+            15.0, 1000, 128, 768, 0.01, 0.03, args.serving_wall, budget_bytes=128 << 20,
+            priority_every=4)
 
     # End to end through the reference entry points on a pinned host array.
     e2e = None
