@@ -54,9 +54,11 @@ constexpr int kBatchCourSlots = 16; // Courant accumulator slots per instance
 constexpr int kBatchXMinBlocks = 14;
 // The mixed-precision x-item kernel (two cells per lane) takes the plain mixed
 // x sweep's cap.  It must: the mixed code is built with FMA contraction, and
-// which multiply-adds the assembler fuses depends on the register budget, so
-// the same window under different caps rounds differently.  With equal caps a
-// batched instance is bitwise equal to its single-grid run (tested).
+// which multiply-adds get fused depends on the context the window is compiled
+// in, register budget included, so the same window under different caps
+// rounds differently.  With equal caps a batched instance is bitwise equal to
+// its single-grid run; the tests check it, since any change to the code
+// around the window can break it.
 constexpr int kBatchXMixedMinBlocks = kMixedCellMinBlocks;
 // The same for the mixed-precision y-item kernel (marching, prefetching):
 // uncapped it takes 147 registers (6 CTAs per SM); 7 CTAs is 3% faster per
