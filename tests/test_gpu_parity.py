@@ -296,3 +296,25 @@ def test_random_states_match_oracle(product_lib, oracle, kind, seed, nx, ny, ext
     d.close()
     assert n == 16 and dt == wdts[-1] and t == wt
     assert bitwise_equal(got, want), describe_mismatch(got, want)
+
+
+def test_16384_two_steps_against_the_oracle(product_lib, oracle):
+    """A large grid (16384^2: 268 M cells, 8.6 GB per state buffer; 131,072
+    marching CTAs per y sweep), two steps bit for bit against the oracle on all
+    host cores."""
+    H = make_params(16384, 16384, testcase=0)
+    u0 = init_state(H)
+    p = orc_from_H(oracle, H)
+    want = u0.copy()
+    oracle.oracle_lib().orc_set_threads(os.cpu_count() or 1)
+    n, wdts, wt = oracle.run(p, want, 2)
+    d = Domain(H)
+    d.upload(u0)
+    del u0
+    d.set_clock()
+    d.launch_steps(2)
+    got = d.download()
+    t, n2, dt = d.get_clock()
+    d.close()
+    assert n == n2 == 2 and t == wt
+    assert bitwise_equal(got, want), describe_mismatch(got, want)
