@@ -175,3 +175,23 @@ def test_batch_random_states_equal_single_runs(product_lib, precision):
         got = b.download(s)
         assert bitwise_equal(got, want), (H.nx, H.ny, describe_mismatch(got, want))
     b.close()
+
+
+def test_full_batched_workload_fp64_sampled_bitwise(product_lib):
+    """The batched workload at its full size (256 seeded instances, sides
+    64..1024, 100 steps each) in FP64: every instance finishes its 100 steps,
+    and every 16th equals its single-grid run bit for bit."""
+    mix = make_blast_mix(256, 20261203)
+    arena = sum(Batch.bytes_needed(H) for H, _ in mix) + (1 << 20)
+    b = Batch(mix[0][0], capacity=256, arena_bytes=arena, precision="fp64")
+    slots = [b.add(H, u, nstepmax=100) for H, u in mix]
+    b.autotune(steps=1)
+    while b.global_step < 110:
+        b.steps(16)
+    active, nstep, _ = b.table()
+    assert all(nstep[s] == 100 and not active[s] for s in slots)
+    for i in range(0, 256, 16):
+        H, u0 = mix[i]
+        want, _, _ = alone(H, u0, 100, "fp64")
+        assert bitwise_equal(b.download(slots[i]), want), (i, H.nx, H.ny)
+    b.close()
