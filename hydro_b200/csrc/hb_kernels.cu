@@ -40,6 +40,42 @@ xcell_kernel(const SweepArgs a, const Phys P) {
     xcell_body<ExactStages<UNIT>>(a, P);
 }
 
+// The y sweep with one cell per lane (lanes along a column): for grids too
+// small to fill the GPU with marching segments, every cell of a window is
+// computed at once instead of one after another.  Same stage calls on the
+// same inputs as the marcher, so the same bits.
+template <bool UNIT>
+__global__ void __launch_bounds__(kCellThreads, kFp64CellMinBlocks)
+ycell_kernel(const SweepArgs a, const Phys P) {
+    const int win = blockIdx.y * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int line = blockIdx.x;
+    bool active = line < a.nlines;
+    double dt = a.dt;
+    if (a.clk) {
+        active = active && a.clk->active;
+        dt = a.clk->dt;
+    }
+    double cx = 0.0, cy = 0.0;
+    if (active) {
+        const typename ExactStages<UNIT>::Consts C = ExactStages<UNIT>::consts(P);
+        line_window_1<ExactStages<UNIT>, 2>(a, C, line, win, dt / P.dx, cx, cy);
+    }
+    if (a.courant) {
+        const int slot = cour_slot();
+        warp_max_atomic(&a.courant[slot], cx);
+        warp_max_atomic(&a.courant[kCourSlots + slot], cy);
+    }
+}
+
+cudaError_t launch_ycell(const SweepArgs& a, const Phys& P, cudaStream_t s) {
+    const int nwin = (a.n - 2 + kCellWarpOut - 1) / kCellWarpOut;
+    const int wpc = kCellThreads / 32;
+    const dim3 grid(a.nlines, (nwin + wpc - 1) / wpc);
+    if (P.unit_slope) ycell_kernel<true><<<grid, kCellThreads, 0, s>>>(a, P);
+    else ycell_kernel<false><<<grid, kCellThreads, 0, s>>>(a, P);
+    return cudaGetLastError();
+}
+
 static dim3 xcell_grid(const SweepArgs& a) {
     // Windows [28w, 28w + 28) cover the outputs [2, n - 2).
     const int nwin = (a.n - 2 + kCellWarpOut - 1) / kCellWarpOut;

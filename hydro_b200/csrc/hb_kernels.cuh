@@ -69,6 +69,7 @@ constexpr int kCellWarpOut2 = 60;  // the same with two cells per lane
 template <class S>
 constexpr int window_out() { return S::cells_per_lane == 2 ? kCellWarpOut2 : kCellWarpOut; }
 cudaError_t launch_xcell(const SweepArgs& a, const Phys& P, cudaStream_t s);
+cudaError_t launch_ycell(const SweepArgs& a, const Phys& P, cudaStream_t s);
 cudaError_t launch_xcell_mixed(const SweepArgs& a, const Phys& P, cudaStream_t s);
 // The mixed-precision sweep (hb_mixed.cu).
 cudaError_t launch_sweep_mixed(int dir, const SweepArgs& a, const Phys& P, cudaStream_t s);

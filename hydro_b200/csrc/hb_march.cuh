@@ -293,15 +293,16 @@ __device__ __forceinline__ F flux_up(const F& f) {
 }
 
 
-// One warp's window: row `row`, output cells [c, c + 28) n [2, n - 2) with
-// c = 28 * win, computed from cells [c - 2, c + 30) (one per lane).  Windows
-// start at multiples of 28 cells (7 sectors of 4 doubles), so when the row
-// pitch is a multiple of 4 cells no 32-byte sector is written by two warps.
-// Accumulates the fused Courant maxima of its outputs into cx, cy.  The
-// caller guarantees the warp is converged and `row` < a.nlines.
-template <class S>
-__device__ __forceinline__ void xcell_window_1(const SweepArgs& a, const typename S::Consts& C,
-                                             int row, int win, double dtdx, double& cx,
+// One warp's window: line `row` (DIR 1: a row; DIR 2: a column, with lanes
+// along y), output cells [c, c + 28) n [2, n - 2) with c = 28 * win, computed
+// from cells [c - 2, c + 30) (one per lane).  Along x, windows start at
+// multiples of 28 cells (7 sectors of 4 doubles), so when the row pitch is a
+// multiple of 4 cells no 32-byte sector is written by two warps.  Accumulates
+// the fused Courant maxima of its outputs into cx, cy.  The caller guarantees
+// the warp is converged and `row` < a.nlines.
+template <class S, int DIR>
+__device__ __forceinline__ void line_window_1(const SweepArgs& a, const typename S::Consts& C,
+                                              int row, int win, double dtdx, double& cx,
                                              double& cy) {
     using Prim = typename S::Prim;
     using Flux = typename S::Flux;
@@ -310,10 +311,10 @@ __device__ __forceinline__ void xcell_window_1(const SweepArgs& a, const typenam
     const int c = win * kCellWarpOut;                // first output cell of the warp
     if (c >= a.n - 2) return;                        // warp-uniform
     const int k = c - 2 + lane;                      // this lane's cell
-    const LineGeom<1> g(a, row);
+    const LineGeom<DIR> g(a, row);
     const typename S::TraceK K = S::trace_constants(C, dtdx);
     const bool inside = k >= 0 && k < a.n;           // lanes outside the row idle
-    const Cons u = inside ? load_cell<1>(a, g, k) : Cons{1.0, 0.0, 0.0, 1.0};
+    const Cons u = inside ? load_cell<DIR>(a, g, k) : Cons{1.0, 0.0, 0.0, 1.0};
     Prim q;
     Real cs;
     S::prim(C, u, q, cs);
@@ -327,14 +328,26 @@ __device__ __forceinline__ void xcell_window_1(const SweepArgs& a, const typenam
     const Flux f_prev = flux_up(f);                  // interface (k - 1 | k)
     if (lane >= 2 && lane < 2 + kCellWarpOut && k >= 2 && k < a.n - 2) {
         const Cons o = S::update(u, f_prev, f, dtdx);
-        store_cell<1>(a, g, k, o);
+        store_cell<DIR>(a, g, k, o);
         if (a.courant) {
             double cn, ct;
             S::courant(C, o, cn, ct);
-            cx = cx > cn ? cx : cn;
-            cy = cy > ct ? cy : ct;
+            if (DIR == 1) {
+                cx = cx > cn ? cx : cn;
+                cy = cy > ct ? cy : ct;
+            } else {
+                cx = cx > ct ? cx : ct;
+                cy = cy > cn ? cy : cn;
+            }
         }
     }
+}
+
+template <class S>
+__device__ __forceinline__ void xcell_window_1(const SweepArgs& a, const typename S::Consts& C,
+                                             int row, int win, double dtdx, double& cx,
+                                             double& cy) {
+    line_window_1<S, 1>(a, C, row, win, dtdx, cx, cy);
 }
 
 // The same with two cells per lane: lane l holds cells ka = c - 2 + 2l and
