@@ -202,6 +202,34 @@ def dom_state_after(H, u0, nsteps, precision):
     return u
 
 
+def mixed_beside_reference_fp32():
+    """Context for the mixed form's error.  The reference's own all-FP32 build
+    (its SP=O option, -DPREC_SP; oracle/_ref/libhydroref_sp.so) and the mixed
+    form are each compared with the FP64 path, which is bitwise equal to the
+    reference's FP64 build, on the same inputs."""
+    from hydro_b200 import init_state, make_params
+    from oracle import oracle as O
+    if not O.ref_available(sp=True):
+        return {"unavailable": "oracle/_ref/libhydroref_sp.so not built"}
+    out = []
+    for label, nx, ny, tc, n in (("250x125 corner blast, 100 steps", 250, 125, 1, 100),
+                                 ("1024x1024 centred blast, 200 steps", 1024, 1024, 0, 200)):
+        H = make_params(nx, ny, testcase=tc)
+        u0 = init_state(H, tc)
+        fp64 = dom_state_after(H, u0, n, "fp64")
+        mix = dom_state_after(H, u0, n, "mixed")
+        with quiet_stdout():  # the reference prints its set-up
+            sp = O.RefState(O.make_param(nx, ny, dx=H.dx), tc, sp=True)
+            sp.set(u0)
+            nsp = sp.run(n)[0]
+            usp = sp.get()
+            sp.close()
+        out.append({"case": label, "steps": nsp,
+                    "mixed_vs_fp64": field_errors(mix, fp64),
+                    "reference_fp32_build_vs_fp64": field_errors(usp, fp64)})
+    return out
+
+
 def run_vtk_form(H, u):
     """One VTK output of the state `u` (the output path, vtkfile.c:140-352):
     the library's vtkfile, which encodes on the GPU from the device mirror.
@@ -632,6 +660,8 @@ def main():
                           "speedup_vs_fp64": round(ms_max / mix_ms, 3),
                           "errors_vs_fp64": err,
                           "precision": "FP32 stages; FP64 Newton p*, update, Courant"}
+        if rank == 0 and world == 1:
+            forms["mixed"]["beside_reference_fp32_build"] = mixed_beside_reference_fp32()
         del ref_state, mix_state
 
     if not args.no_vtk and rank == 0 and world == 1:

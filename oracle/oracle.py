@@ -7,7 +7,10 @@ legs import this module.  It loads
   HydroC99_2Domp time step; built on demand with gcc (``make -C oracle``);
 * ``_ref/libhydroref.so`` -- the reference's own objects behind a small harness
   (oracle/ref_shim.c), present only where the reference sources were available
-  to compile (``make -C oracle ref``).
+  to compile (``make -C oracle ref``);
+* ``_ref/libhydroref_sp.so`` -- the same objects built single precision
+  (the reference's ``SP=O`` option, ``-DPREC_SP``), the context figure for the
+  mixed-precision form's error against FP64.
 
 Both take the same flat parameter record (oracle/orc_param.h).
 """
@@ -23,6 +26,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_ORACLE = os.path.join(HERE, "_build", "liboracle.so")
 _LIB_REF = os.path.join(HERE, "_ref", "libhydroref.so")
+_LIB_REF_SP = os.path.join(HERE, "_ref", "libhydroref_sp.so")
 _lock = threading.Lock()
 
 
@@ -61,7 +65,7 @@ def _build_oracle():
 
 
 _oracle = None
-_ref = None
+_ref: dict = {}
 
 
 def oracle_lib():
@@ -87,15 +91,16 @@ def oracle_lib():
     return _oracle
 
 
-def ref_available() -> bool:
-    return os.path.exists(_LIB_REF)
+def ref_available(sp: bool = False) -> bool:
+    return os.path.exists(_LIB_REF_SP if sp else _LIB_REF)
 
 
-def ref_lib():
-    global _ref
+def ref_lib(sp: bool = False):
+    """The reference harness; ``sp`` selects the single-precision build.  The
+    state crosses it as doubles either way."""
     with _lock:
-        if _ref is None:
-            lib = C.CDLL(_LIB_REF)
+        if sp not in _ref:
+            lib = C.CDLL(_LIB_REF_SP if sp else _LIB_REF)
             lib.ref_create.argtypes = [_P, C.c_int, C.c_int]
             lib.ref_create.restype = C.c_void_p
             lib.ref_destroy.argtypes = [C.c_void_p]
@@ -112,8 +117,11 @@ def ref_lib():
             lib.ref_run.restype = C.c_int
             lib.ref_param_layout.argtypes = [C.POINTER(C.c_long), C.c_int]
             lib.ref_param_layout.restype = C.c_int
-            _ref = lib
-    return _ref
+            lib.ref_real_size.restype = C.c_int
+            if lib.ref_real_size() != (4 if sp else 8):
+                raise RuntimeError(f"{lib._name}: real_t of {lib.ref_real_size()} bytes")
+            _ref[sp] = lib
+    return _ref[sp]
 
 
 def state_shape(p: OrcParam):
@@ -163,9 +171,9 @@ def run(p: OrcParam, u: np.ndarray, nstepmax: int, tend: float = 1e300, threads:
 class RefState:
     """The reference's own state, work space and driver loop (oracle/_ref)."""
 
-    def __init__(self, p: OrcParam, testcase: int, nxystep: int = -1):
+    def __init__(self, p: OrcParam, testcase: int, nxystep: int = -1, sp: bool = False):
         self.p = p
-        self.lib = ref_lib()
+        self.lib = ref_lib(sp)
         self.h = self.lib.ref_create(C.byref(p), testcase, nxystep)
 
     def get(self) -> np.ndarray:

@@ -105,19 +105,23 @@ long ref_ncells(void *h) {
     return (long)s->H.nvar * s->H.nxt * s->H.nyt;
 }
 
+/* The state crosses the harness as doubles whatever real_t is (the single-
+ * precision build, -DPREC_SP, converts on the way in and out). */
 void ref_get(void *h, double *out) {
     ref_state_t *s = (ref_state_t *)h;
-    memcpy(out, s->Hv.uold, sizeof(double) * ref_ncells(h));
+    const long n = ref_ncells(h);
+    for (long i = 0; i < n; i++) out[i] = (double)s->Hv.uold[i];
 }
 
 void ref_set(void *h, const double *in) {
     ref_state_t *s = (ref_state_t *)h;
-    memcpy(s->Hv.uold, in, sizeof(double) * ref_ncells(h));
+    const long n = ref_ncells(h);
+    for (long i = 0; i < n; i++) s->Hv.uold[i] = (real_t)in[i];
 }
 
 double ref_compute_deltat(void *h) {
     ref_state_t *s = (ref_state_t *)h;
-    double dt = 0;
+    real_t dt = 0;
     compute_deltat(&dt, s->H, &s->Hw_deltat, &s->Hv, &s->Hvw_deltat);
     return dt;
 }
@@ -140,7 +144,8 @@ int ref_run(void *h, int nstepmax, double tend, double *dts, double *t_out, doub
             double *elapsed) {
     ref_state_t *s = (ref_state_t *)h;
     hydroparam_t *H = &s->H;
-    double dt = 0, sum = 0;
+    real_t dt = 0;
+    double sum = 0;
     long nsum = 0;
     int n0 = H->nstep;
     double t_start = now_s();
@@ -170,6 +175,9 @@ int ref_run(void *h, int nstepmax, double tend, double *dts, double *t_out, doub
     if (elapsed) *elapsed = now_s() - t_start;
     return H->nstep - n0;
 }
+
+/* real_t of this build: 8 (double) or 4 (-DPREC_SP). */
+int ref_real_size(void) { return (int)sizeof(real_t); }
 
 /* Struct layout of hydroparam_t as the reference compiles it: size and the
  * offset of every field, for the ABI-compatibility test of include/. */

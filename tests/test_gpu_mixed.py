@@ -98,3 +98,31 @@ def test_mixed_random_states(product_lib, capsys, kind, seed, l1):
         print(f"\nrandom {kind}: mixed vs fp64 {err}")
     if l1 is not None:
         assert err["rho"]["l1_rel"] <= l1 and err["E"]["l1_rel"] <= l1, err
+
+
+@pytest.mark.parametrize("nx,ny,tc,nsteps,noise", [(250, 125, 1, 100, False),
+                                                  (512, 512, 1, 300, True)])
+def test_mixed_beside_reference_fp32_build(product_lib, capsys, nx, ny, tc, nsteps, noise):
+    """The mixed form and the reference's own all-FP32 build (SP=O,
+    -DPREC_SP), each against the FP64 path on the same input, printed for the
+    record.  Measured on the 250x125 corner blast: L1 density 5.38e-9 (mixed)
+    against 5.37e-9 (FP32 build), energy 4.1e-7 against 3.7e-7 -- the error
+    comes from the FP32 stages the two share.  Both stay within the
+    north-star bound."""
+    from oracle import oracle as O
+    if not O.ref_available(sp=True):
+        pytest.skip("single-precision reference not compiled (oracle/_ref)")
+    H = make_params(nx, ny, testcase=tc)
+    u0 = init_noisy_blast(H, 20261203, testcase=tc) if noise else init_state(H, tc)
+    ref, _ = run(H, u0, nsteps, "fp64")
+    mix, _ = run(H, u0, nsteps, "mixed")
+    sp = O.RefState(O.make_param(nx, ny, dx=H.dx), tc, sp=True)
+    sp.set(u0)
+    assert sp.run(nsteps)[0] == nsteps
+    usp = sp.get()
+    sp.close()
+    e_mix, e_sp = field_errors(mix, ref), field_errors(usp, ref)
+    with capsys.disabled():
+        print(f"\n{nx}x{ny}: mixed vs fp64 {e_mix}\n{nx}x{ny}: reference FP32 build vs fp64 {e_sp}")
+    for e in (e_mix, e_sp):
+        assert e["rho"]["l1_rel"] <= L1_BOUND and e["E"]["l1_rel"] <= L1_BOUND, (e_mix, e_sp)

@@ -127,3 +127,28 @@ def test_restatement_matches_reference_on_random_states(oracle, kind, seed, extr
     assert np.all(np.isfinite(u))
     assert n == n2 and bitwise_equal(dts, dts2)
     assert bitwise_equal(u, ur), describe_mismatch(u, ur)
+
+
+@pytest.mark.skipif(
+    not __import__("oracle.oracle", fromlist=["x"]).ref_available(sp=True),
+    reason="single-precision reference not compiled here (oracle/_ref)")
+def test_reference_fp32_build_is_a_single_precision_run(oracle):
+    """The reference's all-FP32 build (SP=O, -DPREC_SP), the context figure
+    for the mixed form's error: on the 250x125 corner blast (100 steps) its
+    state holds float32 values only and stays within single-precision
+    distance of the FP64 build, dt sequence included."""
+    from hydro_b200.metrics import field_errors
+    p = oracle.make_param(250, 125)
+    a, b = oracle.RefState(p, 1), oracle.RefState(p, 1, sp=True)
+    na, da, *_ = a.run(100)
+    nb, db, *_ = b.run(100)
+    ua, ub = a.get(), b.get()
+    a.close()
+    b.close()
+    assert na == nb == 100
+    assert np.array_equal(ub, ub.astype(np.float32).astype(np.float64))
+    assert not np.array_equal(ua, ua.astype(np.float32).astype(np.float64))
+    np.testing.assert_allclose(db, da, rtol=1e-5)
+    err = field_errors(ub, ua)
+    for v in ("rho", "E"):
+        assert 0 < err[v]["l1_rel"] < 1e-5, err
