@@ -16,7 +16,7 @@ library's stream; `e2e` is the same metric through the reference entry
 points (compute_deltat + hydro_godunov) on a pinned host array, with the
 upload, the per-step dt reads and the final download inside the timed region.
 With N > 1 (torchrun) every rank advances its own replica (weak scaling; the
-north-star workload is one grid on one GPU, so there is no exchange).
+workload is one grid on one GPU, so there is no exchange).
 
 --impl reference times the reference's own C99/OpenMP implementation of the
 same step on the host cores (oracle/_ref, compiled from the reference
@@ -41,14 +41,14 @@ sys.path.insert(0, ROOT)
 from hydro_b200.metrics import field_errors  # noqa: E402
 
 WORKLOADS = {
-    "c1": dict(name="hydroc_4096x4096_centre_blast_fp64", nx=4096, ny=4096, testcase=0,
-               run_steps=200),
-    "c0": dict(name="hydroc_250x125_corner_blast_fp64", nx=250, ny=125, testcase=1,
-               run_steps=100),
+    "centre_4096": dict(name="hydroc_4096x4096_centre_blast_fp64", nx=4096, ny=4096, testcase=0,
+                        run_steps=200),
+    "corner_250x125": dict(name="hydroc_250x125_corner_blast_fp64", nx=250, ny=125,
+                           testcase=1, run_steps=100),
     # The same problem at 2048^2 (134 MB per state buffer, still > L2): the
     # size the ncu section captures use.
-    "c1_2048": dict(name="hydroc_2048x2048_centre_blast_fp64", nx=2048, ny=2048, testcase=0,
-                    run_steps=200),
+    "centre_2048": dict(name="hydroc_2048x2048_centre_blast_fp64", nx=2048, ny=2048, testcase=0,
+                        run_steps=200),
 }
 BYTES_PER_CELL_SWEEP = 64   # 4 doubles read + 4 doubles written per cell and sweep
 BYTES_PER_CELL_STEP = 2 * BYTES_PER_CELL_SWEEP
@@ -551,7 +551,7 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c1")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="centre_4096")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
@@ -719,7 +719,7 @@ def main():
     if rank != 0:
         return 0
     # The committed ncu traffic figure is for the 4096^2 workload only.
-    traffic = ncu_traffic_per_launch() if args.workload == "c1" else None
+    traffic = ncu_traffic_per_launch() if args.workload == "centre_4096" else None
     line = {
         "metric": "Mcell-updates/s", "value": round(value, 3), "unit": "Mcell-updates/s",
         "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": round(ms_max / K, 4),

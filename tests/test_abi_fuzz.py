@@ -1,7 +1,7 @@
 """Argument validation of the C ABI under random parameter records, on the
 CPU: every entry point either rejects the record with HB_ERR_ARG or gets as
 far as needing a device (HB_ERR_NODEV / HB_ERR_CUDA here, where there is
-none) -- never a crash, never a different verdict from the rules below."""
+none) -- never a crash, never a different outcome from the rules below."""
 import ctypes as C
 
 import pytest
@@ -37,7 +37,7 @@ def admissible(H):
        scheme=st.integers(-1, 5), niter=st.integers(-3, 12),
        dx=st.sampled_from([1e-3, 0.0, -1.0, float("nan"), float("inf"), 1e-300]),
        nxt=st.sampled_from([0, 0, -1, 7]))
-def test_domain_create_verdict(product_lib, nx, ny, nvar, scheme, niter, dx, nxt):
+def test_domain_create_outcome(product_lib, nx, ny, nvar, scheme, niter, dx, nxt):
     H = make_params(8, 8)
     H.nx, H.ny, H.nvar, H.scheme, H.niter_riemann, H.dx = nx, ny, nvar, scheme, niter, dx
     H.nxt = H.nyt = nxt

@@ -1,6 +1,6 @@
 """The mixed-precision form (FP32 stages, FP64 Newton / update / Courant)
 against the FP64 path on the same input: relative L1 density and energy error
-<= 1e-5, conservation with reflecting walls, and
+<= 1e-5 (the required bound), conservation with reflecting walls, and
 agreement of the dt sequence to FP32-level accuracy."""
 import math
 
@@ -75,7 +75,7 @@ def test_mixed_conserves_mass_and_energy(product_lib):
 
 @pytest.mark.parametrize("kind,seed,l1", [("smooth", 33, 1e-5), ("rough", 31, None)])
 def test_mixed_random_states(product_lib, capsys, kind, seed, l1):
-    """Random states (see _helpers.random_state).  Smooth: the north-star
+    """Random states (see _helpers.random_state).  Smooth: the required
     bound against the FP64 path.  Rough (independent cells, shocks and
     rarefactions everywhere, negative internal energies): finite, and mass
     and energy conserved with reflecting walls to FP32 rounding -- the mirror
@@ -108,7 +108,7 @@ def test_mixed_beside_reference_fp32_build(product_lib, capsys, nx, ny, tc, nste
     record.  Measured on the 250x125 corner blast: L1 density 5.38e-9 (mixed)
     against 5.37e-9 (FP32 build), energy 4.1e-7 against 3.7e-7 -- the error
     comes from the FP32 stages the two share.  Both stay within the
-    north-star bound."""
+    required L1 bound."""
     from oracle import oracle as O
     if not O.ref_available(sp=True):
         pytest.skip("single-precision reference not compiled (oracle/_ref)")

@@ -2,7 +2,7 @@
 
 The FP64 kernels round every operation once in the reference's order, so the
 comparison is bitwise: the state (interior AND ghost cells) and every dt.
-The north-star tolerance (1e-12 relative per cell over the run) is therefore
+The required tolerance (1e-12 relative per cell over the run) is therefore
 met with margin 0; the tests assert bit equality and report the first
 mismatch otherwise.
 """

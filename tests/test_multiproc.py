@@ -70,7 +70,7 @@ REF_ARM = r"""
 import sys
 sys.path.insert(0, sys.argv[1])
 sys.argv = ["bench.py", "--impl", "reference", "--steps", "2", "--warmup", "1",
-            "--workload", "c0"]
+            "--workload", "corner_250x125"]
 import bench
 import os
 os.environ["HYDRO_BENCH_REF_BUDGET_S"] = "1"
