@@ -581,9 +581,6 @@ static int ensure_dts(hb_domain* d, int n) {
     return HB_OK;
 }
 
-// Asynchronous: per step one clock kernel (dt on even steps, stop test), the
-// two sweeps (Courant reduction fused into the second sweep of odd steps) and
-// one clock kernel (t += dt, nstep++).
 // What the captured step pair's launches are built from: kernel arguments are
 // captured by value, so any change here needs a new capture.
 static std::vector<unsigned char> pair_key(const hb_domain* d) {
@@ -651,6 +648,9 @@ static int ensure_pair_graph(hb_domain* d) {
     return HB_OK;
 }
 
+// Asynchronous: per step one clock kernel (dt on even steps, stop test), the
+// two sweeps (Courant reduction fused into the second sweep of odd steps) and
+// one clock kernel (t += dt, nstep++).
 extern "C" int hydro_b200_domain_launch_steps(hb_domain* d, int nsteps, int nstepmax,
                                               double tend) {
     if (!d) return set_error(HB_ERR_ARG, "null domain");
