@@ -97,3 +97,18 @@ def test_errors_are_reported_not_fatal(product_lib):
     assert not product_lib.hydro_b200_domain_create(C.byref(H))
     assert product_lib.hydro_b200_last_error() == _lib.HB_ERR_ARG
     product_lib.hydro_b200_clear_error()
+
+
+def test_missing_library_fails_loudly(tmp_path):
+    """Without the built library the package raises: it has no CPU path to
+    fall back on.  Run in a child so this process keeps its loaded library."""
+    code = (
+        "from hydro_b200 import _lib, make_params, Domain\n"
+        f"_lib.LIB_PATH = {str(tmp_path / 'libhydro_b200.so')!r}\n"
+        "try:\n"
+        "    Domain(make_params(32, 32))\n"
+        "except _lib.HydroB200Error as e:\n"
+        "    assert 'no CPU fallback' in str(e), e\n"
+        "    print('raised')\n")
+    r = subprocess.run(["python", "-c", code], capture_output=True, text=True, cwd=ROOT)
+    assert r.returncode == 0 and r.stdout.strip() == "raised", (r.stdout, r.stderr)
