@@ -155,7 +155,7 @@ dist.destroy_process_group()
 """
 
 
-@pytest.mark.parametrize("world,gx,gy,tc", [(2, 41, 27, 0), (4, 36, 30, 1)])
+@pytest.mark.parametrize("world,gx,gy,tc", [(2, 41, 27, 0), (3, 50, 23, 2), (4, 36, 30, 1)])
 def test_gloo_ranks_split_equals_single_grid(tmp_path, world, gx, gy, tc):
     out = str(tmp_path / "g.npy")
     outs = run_ranks(WORKER, world=world, extra_args=(str(gx), str(gy), str(tc), "16", out))
