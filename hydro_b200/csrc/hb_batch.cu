@@ -100,7 +100,7 @@ struct hb_batch {
     hb::Phys P{};
     double courant_factor = 0.8;
     cudaStream_t stream = nullptr;
-    int device = 0, sm_count = 148;
+    int device = 0, sm_count = 0;  // cudaDevAttrMultiProcessorCount, read at creation
     // slots
     std::vector<BatchInst> h;        // host copy of the table
     std::vector<long long> off;      // arena offset (units) of each slot, -1 when free

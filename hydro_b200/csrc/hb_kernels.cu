@@ -129,11 +129,26 @@ int sweep_blocks_per_sm(int dir, bool unit_slope) {
     return (e == cudaSuccess && n > 0) ? n : 1;
 }
 
+int device_sm_count() {
+    // Cached per device: the attribute does not change while the process runs.
+    static int cache[64] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 1;
+    if (cache[dev] == 0) {
+        int n = 0;
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n < 1)
+            return 1;
+        cache[dev] = n;
+    }
+    return cache[dev];
+}
+
 cudaError_t launch_courant(const double* u, int nx, int ny, int nxt, long long vs, const Phys& P,
                            unsigned long long* cour, cudaStream_t s) {
     const long long total = (long long)nx * ny;
     long long blocks = (total + 255) / 256;
-    if (blocks > 148 * 8) blocks = 148 * 8;
+    const long long cap = 8ll * device_sm_count();  // 8 resident CTAs of 256 threads per SM
+    if (blocks > cap) blocks = cap;
     if (blocks < 1) blocks = 1;
     courant_kernel<<<(unsigned)blocks, 256, 0, s>>>(u, nx, ny, nxt, vs, P, cour);
     return cudaGetLastError();
@@ -381,7 +396,8 @@ cudaError_t launch_blast_init(double* u, int nx, int ny, double rho, double ebg,
                               double eblast, cudaStream_t s) {
     const long long vs = (long long)(nx + 4) * (ny + 4);
     long long blocks = (vs + 255) / 256;
-    if (blocks > 148 * 16) blocks = 148 * 16;
+    const long long cap = 16ll * device_sm_count();
+    if (blocks > cap) blocks = cap;
     blast_init_kernel<<<(unsigned)blocks, 256, 0, s>>>(u, nx, ny, rho, ebg, bi, bj, eblast);
     return cudaGetLastError();
 }

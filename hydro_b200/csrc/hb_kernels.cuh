@@ -46,6 +46,10 @@ constexpr int kSweepThreads = 64;
 // slots (max is exact, so the result does not depend on the split).
 constexpr int kCourSlots = 128;
 
+// Multiprocessor count of the current device (cudaDevAttrMultiProcessorCount,
+// cached per device; 1 if it cannot be read).
+int device_sm_count();
+
 // Launchers (hb_kernels.cu).  Each returns the cudaError_t of the launch.
 cudaError_t launch_sweep(int dir, const SweepArgs& a, const Phys& P, cudaStream_t s);
 // Resident sweep CTAs per SM (cudaOccupancyMaxActiveBlocksPerMultiprocessor).

@@ -70,7 +70,8 @@ cudaError_t launch_courant_mixed(const double* u, int nx, int ny, int nxt, long 
                                  const Phys& P, unsigned long long* cour, cudaStream_t s) {
     const long long total = (long long)nx * ny;
     long long blocks = (total + 255) / 256;
-    if (blocks > 148 * 8) blocks = 148 * 8;
+    const long long cap = 8ll * device_sm_count();  // 8 resident CTAs of 256 threads per SM
+    if (blocks > cap) blocks = cap;
     if (blocks < 1) blocks = 1;
     courant_mixed_kernel<<<(unsigned)blocks, 256, 0, s>>>(u, nx, ny, nxt, vs, P, cour);
     return cudaGetLastError();

@@ -86,7 +86,7 @@ struct hb_domain {
     Phys P{};
     double courant_factor = 0.0;
     int bnd_left = 1, bnd_right = 1, bnd_down = 1, bnd_up = 1;
-    int sm_count = 148;
+    int sm_count = 0;  // cudaDevAttrMultiProcessorCount, read in domain_alloc
     int precision = HB_PREC_FP64;
     int xsweep[2] = {HB_XSWEEP_CELL, HB_XSWEEP_CELL};  // x-sweep kernel per precision
     int seg[2][3] = {{0, 64, 64}, {0, 64, 64}};  // [precision][direction] segment lengths
@@ -790,6 +790,46 @@ extern "C" int hydro_b200_release(hydrovar_t* Hv) {
     return HB_OK;
 }
 
+// The reference's per-stage timer table (parametres.h:150-165, defined by the
+// driver at main.c:34 and printed at main.c:515-530).  Weak: it resolves to
+// the driver's table when the library is linked into the reference
+// application, and to null in any other process.
+extern "C" double functim[] __attribute__((weak));
+// Slots of the Timers_t enumeration (parametres.h:150-163) the library fills.
+static constexpr int kTimRieman = 6;   // TIM_RIEMAN: the fused sweeps (all stages)
+static constexpr int kTimMakbou = 10;  // TIM_MAKBOU: make_boundary on its own
+
+// With the driver's timer table present, the entry points time their kernels
+// with CUDA events, wait for them (so that the driver's own clock around the
+// next call does not absorb this call's device time) and add the seconds to
+// functim[slot], as each reference stage adds its own (e.g. riemann.c:287).
+struct StageTimer {
+    hb_domain* d;
+    int slot;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    StageTimer(hb_domain* dom, int s) : d(dom), slot(s) {
+        if (!functim) return;
+        e0 = take_event(d);
+        e1 = take_event(d);
+        if (e0 && e1) cudaEventRecord(e0, d->stream);
+    }
+    void done() {
+        if (!functim || !e0 || !e1) return;
+        float ms = 0.f;
+        if (cudaEventRecord(e1, d->stream) == cudaSuccess &&
+            cudaEventSynchronize(e1) == cudaSuccess &&
+            cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess)
+            functim[slot] += ms * 1e-3;
+        release();
+    }
+    void release() {
+        if (e0) d->ev_pool.push_back(e0);
+        if (e1) d->ev_pool.push_back(e1);
+        e0 = e1 = nullptr;
+    }
+    ~StageTimer() { release(); }
+};
+
 extern "C" void hydro_godunov(int idim, real_t dt, const hydroparam_t H, hydrovar_t* Hv,
                               hydrowork_t* Hw, hydrovarwork_t* Hvw) {
     (void)Hw;
@@ -802,7 +842,9 @@ extern "C" void hydro_godunov(int idim, real_t dt, const hydroparam_t H, hydrova
     }
     // The reference driver calls compute_deltat right after every idim == 2
     // step (main.c:349-399): reduce the Courant maxima inside its second sweep.
+    StageTimer tim(d, kTimRieman);
     if (domain_step(d, idim, dt, nullptr, idim == 2) != HB_OK) return;
+    tim.done();
     if (sync_each_call()) {
         if (hydro_b200_domain_download(d, Hv->uold) == HB_OK) hydro_b200_domain_synchronize(d);
     }
@@ -829,7 +871,9 @@ extern "C" void compute_deltat(real_t* dt, const hydroparam_t H, hydrowork_t* Hw
 extern "C" void make_boundary(int idim, const hydroparam_t H, hydrovar_t* Hv) {
     hb_domain* d = mirror_for(&H, Hv);
     if (!d) return;
+    StageTimer tim(d, kTimMakbou);  // make_boundary.c:202
     if (hydro_b200_domain_make_boundary(d, idim) != HB_OK) return;
+    tim.done();
     if (sync_each_call()) {
         if (hydro_b200_domain_download(d, Hv->uold) == HB_OK) hydro_b200_domain_synchronize(d);
     }

@@ -313,18 +313,24 @@ int hydro_b200_batch_autotune(hb_batch *b, int steps);
 int hydro_b200_set_device(int device);
 
 /* A hydro_godunov step (FP64, the sweeps of hydro_godunov) for callers that
- * cannot allocate device memory.  No counterpart in the reference.  The
- * caller holds the state on the device (d_uold, reference layout, updated in
- * place) and passes the stream (a cudaStream_t, or NULL); the second buffer
- * the sweeps need is a static __device__ array of 4*HB_NOALLOC_MAX_CELLS
- * doubles (32 MiB) that every GPU loading the library keeps until exit, so the
- * call makes no cudaMalloc / cudaFree / stream or event creation.  Grids with
- * (nx+4)*(ny+4) > HB_NOALLOC_MAX_CELLS are rejected with HB_ERR_ARG.  The
- * first call on a device looks up the array's device address
- * (cudaGetSymbolAddress); make that first call before any stream capture.
- * All calls share the one array: calls whose kernels overlap on the GPU race,
- * so serialise them.  Returns HB_OK or an error code (message in
- * hydro_b200_last_error_message). */
+ * cannot allocate device memory: code running inside another framework's
+ * memory arena, which owns the device memory it hands out, or in a process
+ * whose device-allocation budget is already spent.  No counterpart in the
+ * reference.  The caller holds the state on the device (d_uold, reference
+ * layout, 4*(nx+4)*(ny+4) doubles, updated in place) and passes the stream (a
+ * cudaStream_t, or NULL).  d_uold must be device or managed memory of the
+ * current device (hydro_b200_set_device); anything else, host memory
+ * included, is rejected with HB_ERR_ARG.  The second buffer the sweeps need
+ * is a static __device__ array of 4*HB_NOALLOC_MAX_CELLS doubles (32 MiB)
+ * that every GPU loading the library keeps until exit, so the call makes no
+ * cudaMalloc / cudaFree / stream or event creation.  Grids with
+ * (nx+4)*(ny+4) > HB_NOALLOC_MAX_CELLS are rejected with HB_ERR_ARG.  It runs
+ * the kernels hydro_godunov uses for grids of this size, so the results are
+ * the same bits.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress); make that first call before any stream
+ * capture.  All calls share the one array: calls whose kernels overlap on
+ * the GPU race, so serialise them.  Returns HB_OK or an error code (message
+ * in hydro_b200_last_error_message). */
 #define HB_NOALLOC_MAX_CELLS (1 << 20)
 int hydro_b200_godunov_noalloc(const hydroparam_t *H, double *d_uold, int idim, double dt,
                                void *stream);

@@ -56,20 +56,38 @@ def test_domain_create_outcome(product_lib, nx, ny, nvar, scheme, niter, dx, nxt
 
 
 @settings(max_examples=200, deadline=None)
-@given(nx=INT, ny=INT, idim=st.integers(-1, 3))
-def test_noalloc_rejects_before_touching_memory(product_lib, nx, ny, idim):
-    """The allocation-free entry point checks its arguments before it looks
-    at the (here bogus) state pointer."""
+@given(nx=INT, ny=INT, idim=st.integers(-1, 3), strides=st.sampled_from(["unset", "set", "bad"]))
+def test_noalloc_rejects_before_touching_memory(product_lib, nx, ny, idim, strides):
+    """The allocation-free entry point checks its arguments, then that the
+    state is device memory of the current device, before any launch: here
+    (no device) every call is rejected with HB_ERR_ARG, and the message says
+    which rule failed."""
     H = make_params(8, 8)
     H.nx, H.ny = nx, ny
+    H.nxt, H.nyt = {"unset": (0, 0), "set": (nx + 4, ny + 4), "bad": (nx + 5, ny + 4)}[strides]
     product_lib.hydro_b200_clear_error()
     rc = product_lib.hydro_b200_godunov_noalloc(C.byref(H), C.c_void_p(16), idim, 1e-3, None)
+    msg = product_lib.hydro_b200_last_error_message()
     product_lib.hydro_b200_clear_error()
     too_big = nx >= 3 and ny >= 3 and (nx + 4) * (ny + 4) > _lib.HB_NOALLOC_MAX_CELLS
-    if idim not in (1, 2) or nx < 3 or ny < 3 or too_big:
-        assert rc == _lib.HB_ERR_ARG
+    assert rc == _lib.HB_ERR_ARG
+    if idim not in (1, 2) or nx < 3 or ny < 3 or strides == "bad" or too_big:
+        assert b"not a device pointer" not in msg, msg
     else:
-        assert rc in (_lib.HB_ERR_CUDA, _lib.HB_ERR_NODEV)
+        assert b"not a device pointer" in msg, msg
+
+
+def test_noalloc_rejects_a_host_state(product_lib):
+    """A state in host memory is rejected (HB_ERR_ARG) instead of being handed
+    to kernels that cannot read it."""
+    import numpy as np
+    H = make_params(16, 12)
+    u = np.zeros((4, H.ny + 4, H.nx + 4))
+    product_lib.hydro_b200_clear_error()
+    rc = product_lib.hydro_b200_godunov_noalloc(C.byref(H), u.ctypes.data, 1, 1e-3, None)
+    assert rc == _lib.HB_ERR_ARG
+    assert product_lib.hydro_b200_last_error() == _lib.HB_ERR_ARG
+    product_lib.hydro_b200_clear_error()
 
 
 @settings(max_examples=100, deadline=None)

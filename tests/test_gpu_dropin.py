@@ -51,6 +51,16 @@ NMLS = {
 NML = NML_TEMPLATE.format(**NMLS["corner_250x125"])
 
 
+def timer_line(stdout):
+    """The driver's timer table (main.c:515-525): the label line (GATCON ...
+    ALLRED) and the PE0_DP line of seconds under it, as {label: seconds}."""
+    lines = stdout.splitlines()
+    for k, line in enumerate(lines):
+        if line.startswith("PE0_DP") and k > 0:
+            return dict(zip(lines[k - 1].split(), (float(x) for x in line.split()[1:])))
+    raise AssertionError("no PE0_DP timer line in the driver's output")
+
+
 # hydro_dropin: the reference's own vtkfile.c reads the host array, which the
 # library copies back after every step (HYDRO_B200_SYNC=1).
 # hydro_dropin_vtk: the library's vtkfile writes from the device state; the
@@ -71,8 +81,13 @@ def test_reference_driver_runs_on_the_gpu_path(tmp_path, product_lib, name, sync
         assert r.returncode == 0, r.stderr[-2000:]
         steps = re.findall(r"--> step=\s*(\d+),\s*(\S+),\s*(\S+)", r.stdout)
         assert len(steps) == 60
-        outs[exe] = (d, steps)
+        outs[exe] = (d, steps, r.stdout)
     assert outs["hydro"][1] == outs[name][1]
+    # The driver's per-stage timer line (main.c:515-530): the library adds the
+    # device time of its fused sweeps to TIM_RIEMAN (the driver itself times
+    # compute_deltat into TIM_COMPDT).
+    tim = timer_line(outs[name][2])
+    assert tim["RIEMAN"] > 0.0 and tim["COMPDT"] > 0.0, tim
     a, b = outs["hydro"][0], outs[name][0]
     files = sorted(os.path.relpath(os.path.join(dp, f), a)
                    for dp, _, fs in os.walk(a) for f in fs

@@ -243,8 +243,11 @@ def test_full_size_4096_first_steps_and_conservation(product_lib, oracle):
 def test_full_size_4096_200_steps_against_the_reference(product_lib, oracle):
     """The 4096^2 centred blast over its whole 200-step run, per cell and per
     dt, against the reference's own C99/OpenMP code (oracle/_ref, built from
-    the reference sources; the C restatement where it is absent), run on all
-    host cores."""
+    the reference sources), run on all host cores.  Skipped, not downgraded,
+    where the reference was not compiled."""
+    if not oracle.ref_available():
+        pytest.skip("oracle/_ref (the reference compiled from its sources) is not built: "
+                    "the full-run parity test needs the reference itself")
     H = make_params(4096, 4096, testcase=0)
     u0 = init_state(H)
     run = HydroRun(H, u0.copy())
@@ -253,15 +256,10 @@ def test_full_size_4096_200_steps_against_the_reference(product_lib, oracle):
     t_gpu = run.t
     run.close()
     p = orc_from_H(oracle, H)
-    if oracle.ref_available():
-        ref = oracle.RefState(p, 0)
-        n, wdts, wt, _, _ = ref.run(200)
-        want = ref.get()
-        ref.close()
-    else:
-        oracle.oracle_lib().orc_set_threads(os.cpu_count() or 1)
-        want = u0.copy()
-        n, wdts, wt = oracle.run(p, want, 200)
+    ref = oracle.RefState(p, 0)
+    n, wdts, wt, _, _ = ref.run(200)
+    want = ref.get()
+    ref.close()
     assert n == 200 and len(dts) == 200
     assert bitwise_equal(dts, wdts) and t_gpu == wt
     assert bitwise_equal(got, want), describe_mismatch(got, want)
