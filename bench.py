@@ -51,6 +51,9 @@ WORKLOADS = {
                         run_steps=200),
 }
 BYTES_PER_CELL_SWEEP = 64   # 4 doubles read + 4 doubles written per cell and sweep
+# CUDA kernel of each sweep-kernel choice (FP64 set).
+KERNEL_NAMES = {"march": "sweep_kernel", "warp": "xcell_kernel / ycell_kernel",
+                "coop": "coop_kernel<.,.,4>", "coop8": "coop_kernel<.,.,8>"}
 BYTES_PER_CELL_STEP = 2 * BYTES_PER_CELL_SWEEP
 
 
@@ -230,6 +233,99 @@ def mixed_beside_reference_fp32():
     return out
 
 
+def tier_errors(got, want):
+    """Per-cell errors of the FMA FP64 tier's rule: density and energy
+    relative; momenta relative to the larger of the cell's value and the
+    field's largest magnitude."""
+    out = {}
+    for v, name in enumerate(("rho", "rhou", "rhov", "E")):
+        a, b = got[v], want[v]
+        den = np.abs(b) if name in ("rho", "E") else np.maximum(np.abs(b), np.max(np.abs(b)))
+        err = np.abs(a - b) / np.where(den > 0, den, 1.0)
+        out[name] = float(f"{float(err.max()):.3g}")
+    return out
+
+
+def run_fma_form(H, u0, K, W, ref_state, ref_dts, pg, device, world):
+    """The FMA FP64 tier on the same workload and steps: FP64 throughout with
+    FMA contraction and refined reciprocals; per-cell errors and dt errors
+    against the bit-exact FP64 run (itself bitwise the reference's)."""
+    import torch
+    from hydro_b200 import Domain
+    d = Domain(H, precision="fma")
+    d.upload(u0)
+    d.set_clock()
+    d.launch_steps(W)
+    d.synchronize()
+    d.upload(u0)
+    d.reserve_dts(K)
+    d.set_clock()
+    st = torch.cuda.ExternalStream(d.stream_ptr, device=device)
+    barrier(pg, device)
+    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g0.record(st)
+    d.launch_steps(K)
+    g1.record(st)
+    g1.synchronize()
+    ms = all_max(pg, g0.elapsed_time(g1), device)
+    u = d.download()
+    dts = d.get_dts(K)
+    kern = d.kernels()
+    d.close()
+    dt_rel = float(np.max(np.abs(dts - ref_dts) / ref_dts))
+    return {"value": round(world * H.nx * H.ny * K / (ms / 1e3) / 1e6, 3),
+            "unit": "Mcell-updates/s", "ms_per_step": round(ms / K, 4),
+            "kernels": {"x": kern[0], "y": kern[1]},
+            "max_err_vs_fp64": tier_errors(u, ref_state), "dt_max_rel_vs_fp64": float(f"{dt_rel:.3g}"),
+            "rule": "rho, E relative per cell; momenta relative to max(|cell|, field max); "
+                    "the FP64 run is bitwise the reference's",
+            "precision": "FP64, FMA contraction, refined reciprocals (HB_PREC_FP64_FMA)"}
+
+
+def run_noalloc_form(device):
+    """The allocation-free step against the regular domain step on the same
+    grids (CUDA events, fixed dt, 50 steps each after 5 warm-up steps)."""
+    import ctypes as C
+    import torch
+    from hydro_b200 import Domain, init_state, load, make_params
+    lib = load()
+    out = []
+    for nx, ny in ((250, 125), (1020, 1020)):
+        H = make_params(nx, ny, testcase=1)
+        u0 = init_state(H)
+        dt = 0.4 / max(nx, ny) ** 2
+        d = Domain(H)
+        d.upload(u0)
+        st = torch.cuda.ExternalStream(d.stream_ptr, device=device)
+        for k in range(5):
+            d.godunov(1 + k % 2, dt)
+        d.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for k in range(50):
+            d.godunov(1 + k % 2, dt)
+        e1.record(st)
+        e1.synchronize()
+        reg = e0.elapsed_time(e1) / 50
+        d.close()
+        state = torch.from_numpy(u0).to(device)
+        s2 = torch.cuda.Stream(device=device)
+        h = C.c_void_p(s2.cuda_stream)
+        torch.cuda.synchronize(device)
+        for k in range(5):
+            lib.hydro_b200_godunov_noalloc(C.byref(H), state.data_ptr(), 1 + k % 2, dt, h)
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(s2)
+        for k in range(50):
+            lib.hydro_b200_godunov_noalloc(C.byref(H), state.data_ptr(), 1 + k % 2, dt, h)
+        f1.record(s2)
+        f1.synchronize()
+        na = f0.elapsed_time(f1) / 50
+        out.append({"grid": f"{nx}x{ny}", "noalloc_ms_per_step": round(na, 4),
+                    "regular_ms_per_step": round(reg, 4), "ratio": round(na / reg, 3)})
+    return out
+
+
 def run_vtk_form(H, u):
     """One VTK output of the state `u` (the output path, vtkfile.c:140-352):
     the library's vtkfile, which encodes on the GPU from the device mirror.
@@ -341,6 +437,18 @@ def run_batched_form(device, seed=20261203, n=256, nsteps=100):
                                    **{v: float(f"{x:.3g}") for v, x in worst.items()}}}
 
 
+def serving_accuracy_requests():
+    """A labelled mix for the served results' accuracy at large sides: four
+    requests of side 1024..1536 and four of side 128..256 (tend 0.01, blast
+    parameters drawn as in the stream), arriving within 50 ms, so that they
+    are served together."""
+    from hydro_b200.serve import Request, poisson_requests
+    sides = [1024, 1536, 1280, 1088, 128, 192, 256, 136]
+    base = poisson_requests(len(sides), 100.0, 20261205, 128, 256, 0.01, 0.01)
+    return [Request(k, 0.00625 * k, sides[k], 0.01, r.bx, r.by, r.e0, r.rho)
+            for k, r in enumerate(base)]
+
+
 def solve_fp64(req):
     """A served request solved alone in FP64 until its tend."""
     from hydro_b200 import Batch
@@ -356,7 +464,7 @@ def solve_fp64(req):
 
 
 def run_serving_form(label, rate, n, side_lo, side_hi, tend_lo, tend_hi, wall_s, seed=20261204,
-                     budget_bytes=None, priority_every=0):
+                     budget_bytes=None, priority_every=0, sample_small=6, requests=None):
     """The serving loop (continuous batching) on a Poisson request stream;
     arena = 80% of the free HBM unless budget_bytes is given; time-bounded.
     With priority_every = k, every k-th request has priority 1 (the others 0)
@@ -367,13 +475,16 @@ def run_serving_form(label, rate, n, side_lo, side_hi, tend_lo, tend_hi, wall_s,
     from hydro_b200.serve import BatchBackend, Server, poisson_requests
     free, total = torch.cuda.mem_get_info()
     budget = int(0.8 * free) if budget_bytes is None else int(budget_bytes)
-    reqs = poisson_requests(n, rate, seed, side_lo, side_hi, tend_lo, tend_hi)
+    reqs = requests if requests is not None else poisson_requests(n, rate, seed, side_lo, side_hi,
+                                                                  tend_lo, tend_hi)
     if priority_every:
         reqs = [dataclasses.replace(r, priority=1 if r.rid % priority_every == 0 else 0)
                 for r in reqs]
     # Accuracy of what was served: the first few small requests are kept and
     # compared with their FP64 solves.
-    sample = set([r.rid for r in reqs if r.side <= 256][:6])
+    sample = set([r.rid for r in reqs if r.side <= 256][:sample_small])
+    if requests is not None:
+        sample = set(r.rid for r in reqs)  # an explicit request list: every result is checked
     be = BatchBackend(make_params(128, 128), budget, capacity=4096, keep_results=sample)
     st = Server(be, preempt=bool(priority_every)).run(reqs, max_wall_s=wall_s)
     be.close()
@@ -392,7 +503,8 @@ def run_serving_form(label, rate, n, side_lo, side_hi, tend_lo, tend_hi, wall_s,
         err = field_errors(u, solve_fp64(by_id[rid]))
         for v in worst:
             worst[v] = max(worst[v], err[v]["l1_rel"])
-    out["l1_rel_vs_fp64_max"] = {"sample": f"{len(be.results)} completed requests of side <= 256",
+    sides = sorted(by_id[rid].side for rid in be.results)
+    out["l1_rel_vs_fp64_max"] = {"sample": f"{len(be.results)} completed requests, sides {sides}",
                                  **{v: float(f"{x:.3g}") for v, x in worst.items()}}
     out.update({"label": label, "lambda_per_s": rate, "requests_offered": n,
                 "sides": [side_lo, side_hi], "tend": [tend_lo, tend_hi],
@@ -555,10 +667,13 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-fma", action="store_true")
+    ap.add_argument("--no-noalloc", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-vtk", action="store_true")
-    ap.add_argument("--serving-wall", type=float, default=25.0)
+    ap.add_argument("--serving-wall", type=float, default=20.0)
+    ap.add_argument("--knee-wall", type=float, default=8.0)
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
     if args.warmup < 3:
@@ -627,6 +742,7 @@ def main():
     msx, msy, nxl, nyl = dom.profile_read(reset=True)
     dom.profile(False)
     sweep_ms = (msx + msy) / max(nxl + nyl, 1)
+    kern = dom.kernels()
     alg_bytes = BYTES_PER_CELL_SWEEP * nx * ny
     achieved = alg_bytes / (sweep_ms / 1e3) / 1e9
     peak, peak_kind = measured_peak_hbm()
@@ -635,8 +751,19 @@ def main():
     # The mixed-precision form on the same workload and steps, with its error
     # against the FP64 state.
     forms = {}
+    ref_state = None
+    if not (args.no_mixed and args.no_fma):
+        dref = Domain(H)
+        dref.upload(u0)
+        dref.reserve_dts(K)
+        dref.set_clock()
+        dref.launch_steps(K)
+        ref_state = dref.download()
+        ref_dts = dref.get_dts(K)
+        dref.close()
+    if not args.no_fma:
+        forms["fp64_fma"] = run_fma_form(H, u0, K, W, ref_state, ref_dts, pg, device, world)
     if not args.no_mixed:
-        ref_state = dom_state_after(H, u0, K, "fp64")
         dm = Domain(H, precision="mixed")
         dm.upload(u0)
         dm.set_clock()
@@ -662,8 +789,11 @@ def main():
                           "precision": "FP32 stages; FP64 Newton p*, update, Courant"}
         if rank == 0 and world == 1:
             forms["mixed"]["beside_reference_fp32_build"] = mixed_beside_reference_fp32()
-        del ref_state, mix_state
+        del mix_state
 
+    ref_state = None
+    if not args.no_noalloc and rank == 0 and world == 1:
+        forms["noalloc"] = run_noalloc_form(device)
     if not args.no_vtk and rank == 0 and world == 1:
         forms["vtk_output"] = run_vtk_form(H, dom_state_after(H, u0, min(K, 20), "fp64"))
     if not args.no_batched and rank == 0:
@@ -672,9 +802,16 @@ def main():
         forms["serving"] = run_serving_form(
             "configured stream: lambda 200/s, sides 128..4096, tend 0.01..0.1 (time-bounded)",
             200.0, 10000, 128, 4096, 0.01, 0.1, args.serving_wall)
-        forms["serving_subsaturating"] = run_serving_form(
-            "sub-saturating stream (labelled): lambda 20/s, sides 128..512, tend 0.01..0.03",
-            20.0, 400, 128, 512, 0.01, 0.03, args.serving_wall)
+        # Arrival rates around the knee, where the offered load meets the
+        # batch's throughput (labelled streams of smaller solves).
+        forms["serving_knee"] = [run_serving_form(
+            f"labelled stream: lambda {lam:g}/s, sides 128..512, tend 0.01..0.03",
+            lam, int(lam * args.knee_wall * 1.5) + 10, 128, 512, 0.01, 0.03, args.knee_wall,
+            sample_small=2) for lam in (20.0, 80.0, 160.0, 320.0)]
+        forms["serving_accuracy"] = run_serving_form(
+            "labelled mix: sides 1024..1536 and 128..256, tend 0.01, arriving within 50 ms; "
+            "every result against its FP64 solve", 0.0, 8, 128, 1536, 0.01, 0.01, 60.0,
+            requests=serving_accuracy_requests())
         forms["serving_priority"] = run_serving_form(
             "priority mix (labelled): lambda 15/s, sides 128..768, tend 0.01..0.03, every 4th "
             "request priority 1 with preemption, 128 MB arena (memory-bound on purpose)",
@@ -733,7 +870,8 @@ def main():
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                      "unit": "GB/s", "frac": round(achieved / peak, 4),
                      "traffic": traffic,
-                     "kernel": "xcell_kernel<1> (x sweep) and sweep_kernel<2,1> (y sweep)",
+                     "kernel": f"FP64 sweeps: x {kern[0]} window, y {kern[1]} "
+                               f"({KERNEL_NAMES[kern[0]]} and {KERNEL_NAMES[kern[1]]})",
                      "alg_bytes_per_launch": alg_bytes, "launch_ms": round(sweep_ms, 4),
                      "fp64_pipe": ncu_fp64_pipe(),
                      "peak_kind": peak_kind},

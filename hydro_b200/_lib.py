@@ -18,11 +18,14 @@ LIB_PATH = os.path.join(PKG_DIR, "libhydro_b200.so")
 MAX_BOX = 8
 
 HB_OK, HB_ERR_ARG, HB_ERR_CUDA, HB_ERR_NODEV, HB_ERR_NOMEM, HB_ERR_STATE, HB_ERR_TIMEOUT = range(7)
-HB_PREC_FP64, HB_PREC_MIXED = 0, 1
-PRECISIONS = {"fp64": HB_PREC_FP64, "mixed": HB_PREC_MIXED}
+HB_PREC_FP64, HB_PREC_MIXED, HB_PREC_FP64_FMA = 0, 1, 2
+PRECISIONS = {"fp64": HB_PREC_FP64, "mixed": HB_PREC_MIXED, "fma": HB_PREC_FP64_FMA}
 HB_XSWEEP_MARCH, HB_XSWEEP_CELL = 0, 1
 HB_NOALLOC_MAX_CELLS = 1 << 20  # include/hydro_b200.h
 XSWEEPS = {"march": HB_XSWEEP_MARCH, "cell": HB_XSWEEP_CELL}
+HB_KERNEL_AUTO, HB_KERNEL_MARCH, HB_KERNEL_WARP, HB_KERNEL_COOP, HB_KERNEL_COOP8 = -1, 0, 1, 2, 3
+KERNELS = {"auto": HB_KERNEL_AUTO, "march": HB_KERNEL_MARCH, "warp": HB_KERNEL_WARP,
+           "coop": HB_KERNEL_COOP, "coop8": HB_KERNEL_COOP8}
 
 
 class HydroParam(C.Structure):
@@ -133,9 +136,14 @@ SIGNATURES = [
     ("hydro_b200_domain_launch_steps", C.c_int, [_D, C.c_int, C.c_int, C.c_double]),
     ("hydro_b200_domain_get_clock", C.c_int, [_D, _DP, C.POINTER(C.c_int), _DP]),
     ("hydro_b200_domain_get_dts", C.c_int, [_D, _DP, C.c_int]),
+    ("hydro_b200_domain_reserve_dts", C.c_int, [_D, C.c_int]),
     ("hydro_b200_domain_launch_count", C.c_longlong, [_D]),
     ("hydro_b200_domain_set_precision", C.c_int, [_D, C.c_int]),
     ("hydro_b200_domain_set_xsweep", C.c_int, [_D, C.c_int, C.c_int]),
+    ("hydro_b200_domain_set_kernel", C.c_int, [_D, C.c_int, C.c_int, C.c_int]),
+    ("hydro_b200_domain_sweep_part", C.c_int, [_D, C.c_int, C.c_int, C.c_double, C.c_int,
+                                                C.c_int]),
+    ("hydro_b200_domain_get_kernel", C.c_int, [_D, C.c_int, C.c_int]),
     ("hydro_b200_domain_profile", C.c_int, [_D, C.c_int]),
     ("hydro_b200_domain_profile_read", C.c_int, [_D, _DP, C.POINTER(C.c_longlong), C.c_int]),
     ("hydro_b200_batch_create", _D, [_P, C.c_int, C.c_size_t, C.c_int]),

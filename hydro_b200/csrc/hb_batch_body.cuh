@@ -34,6 +34,8 @@ __device__ __forceinline__ SweepArgs batch_args(const BatchInst& I, int dir, int
         a.n = I.nyt;
     }
     a.seg = 0;
+    a.w_lo = 0;
+    a.w_hi = kWholeLine;
     return a;
 }
 

@@ -24,6 +24,7 @@
 // ends in the resident array after both sweeps.
 #include "hb_kernels.cuh"
 #include "hb_march.cuh"
+#include "hb_coop.cuh"
 #include "hb_batch_body.cuh"
 
 namespace hb {
@@ -47,9 +48,9 @@ xcell_kernel(const SweepArgs a, const Phys P) {
 template <bool UNIT>
 __global__ void __launch_bounds__(kCellThreads, kFp64CellMinBlocks)
 ycell_kernel(const SweepArgs a, const Phys P) {
-    const int win = blockIdx.y * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int win = a.w_lo + blockIdx.y * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int line = blockIdx.x;
-    bool active = line < a.nlines;
+    bool active = line < a.nlines && win < a.w_hi;
     double dt = a.dt;
     if (a.clk) {
         active = active && a.clk->active;
@@ -68,22 +69,53 @@ ycell_kernel(const SweepArgs a, const Phys P) {
 }
 
 cudaError_t launch_ycell(const SweepArgs& a, const Phys& P, cudaStream_t s) {
-    const int nwin = (a.n - 2 + kCellWarpOut - 1) / kCellWarpOut;
+    const int nwin = window_span(a, (a.n - 2 + kCellWarpOut - 1) / kCellWarpOut);
     const int wpc = kCellThreads / 32;
+    if (nwin == 0) return cudaSuccess;
     const dim3 grid(a.nlines, (nwin + wpc - 1) / wpc);
     if (P.unit_slope) ycell_kernel<true><<<grid, kCellThreads, 0, s>>>(a, P);
     else ycell_kernel<false><<<grid, kCellThreads, 0, s>>>(a, P);
     return cudaGetLastError();
 }
 
+// The cooperative window (hb_coop.cuh): a CTA of G warps per 32G cells of a
+// line, register cap as the warp window's (kFp64CellMinBlocks CTAs of 64
+// threads per SM).
+template <bool UNIT, int DIR, int G>
+__global__ void __launch_bounds__(32 * G, kFp64CellMinBlocks * 2 / G)
+coop_kernel(const SweepArgs a, const Phys P) {
+    coop_body<ExactStages<UNIT>, DIR, G>(a, P);
+}
+
+template <int G>
+static cudaError_t launch_coop_g(int dir, const SweepArgs& a, const Phys& P, cudaStream_t s) {
+    const int nwin = window_span(a, coop_windows<G>(a.n));
+    if (nwin == 0) return cudaSuccess;
+    const dim3 grid(a.nlines, nwin);
+    if (dir == 1) {
+        if (P.unit_slope) coop_kernel<true, 1, G><<<grid, 32 * G, 0, s>>>(a, P);
+        else coop_kernel<false, 1, G><<<grid, 32 * G, 0, s>>>(a, P);
+    } else {
+        if (P.unit_slope) coop_kernel<true, 2, G><<<grid, 32 * G, 0, s>>>(a, P);
+        else coop_kernel<false, 2, G><<<grid, 32 * G, 0, s>>>(a, P);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_coop(int dir, int warps, const SweepArgs& a, const Phys& P, cudaStream_t s) {
+    if (warps == 8) return launch_coop_g<8>(dir, a, P, s);
+    return launch_coop_g<4>(dir, a, P, s);
+}
+
 static dim3 xcell_grid(const SweepArgs& a) {
     // Windows [28w, 28w + 28) cover the outputs [2, n - 2).
-    const int nwin = (a.n - 2 + kCellWarpOut - 1) / kCellWarpOut;
+    const int nwin = window_span(a, (a.n - 2 + kCellWarpOut - 1) / kCellWarpOut);
     const int wpc = kCellThreads / 32;
     return dim3(a.nlines, (nwin + wpc - 1) / wpc);
 }
 
 cudaError_t launch_xcell(const SweepArgs& a, const Phys& P, cudaStream_t s) {
+    if (xcell_grid(a).y == 0) return cudaSuccess;
     if (P.unit_slope) xcell_kernel<true><<<xcell_grid(a), kCellThreads, 0, s>>>(a, P);
     else xcell_kernel<false><<<xcell_grid(a), kCellThreads, 0, s>>>(a, P);
     return cudaGetLastError();
@@ -91,7 +123,9 @@ cudaError_t launch_xcell(const SweepArgs& a, const Phys& P, cudaStream_t s) {
 
 cudaError_t launch_sweep(int dir, const SweepArgs& a, const Phys& P, cudaStream_t s) {
     const int nl = a.n - 4;
-    dim3 grid((a.nlines + kSweepThreads - 1) / kSweepThreads, (nl + a.seg - 1) / a.seg);
+    const int nseg = window_span(a, (nl + a.seg - 1) / a.seg);
+    if (nseg == 0) return cudaSuccess;
+    dim3 grid((a.nlines + kSweepThreads - 1) / kSweepThreads, nseg);
     if (dir == 1) {
         if (P.unit_slope) sweep_kernel<1, true><<<grid, kSweepThreads, 0, s>>>(a, P);
         else sweep_kernel<1, false><<<grid, kSweepThreads, 0, s>>>(a, P);

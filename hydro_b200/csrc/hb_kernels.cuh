@@ -35,7 +35,20 @@ struct SweepArgs {
     int seg;                 // output cells per thread segment
     int nlines;              // interior lines (ny for the x sweep, nx for the y sweep)
     int n;                   // cells along a line including ghosts (nxt or nyt)
+    // Windows (segments for the marching kernels) [w_lo, w_hi) of every line
+    // are swept: the launch grid starts at window w_lo.  0 and a large w_hi
+    // sweep the whole line; a domain split sweeps the windows that read no
+    // ghost cell while the halos travel, and the others after.
+    int w_lo, w_hi;
 };
+
+// Windows of [w_lo, w_hi) n [0, total) a launch covers (its grid's y extent
+// in windows; 0: nothing to launch).
+inline int window_span(const SweepArgs& a, int total) {
+    const int hi = a.w_hi < total ? a.w_hi : total;
+    return hi > a.w_lo ? hi - a.w_lo : 0;
+}
+constexpr int kWholeLine = 1 << 30;  // w_hi of a launch over whole lines
 
 constexpr int kSweepThreads = 64;
 
@@ -73,8 +86,18 @@ constexpr int kCellWarpOut2 = 60;  // the same with two cells per lane
 template <class S>
 constexpr int window_out() { return S::cells_per_lane == 2 ? kCellWarpOut2 : kCellWarpOut; }
 cudaError_t launch_xcell(const SweepArgs& a, const Phys& P, cudaStream_t s);
+// The cooperative window (hb_coop.cuh), `warps` = 4 or 8 warps per CTA.
+cudaError_t launch_coop(int dir, int warps, const SweepArgs& a, const Phys& P, cudaStream_t s);
+cudaError_t launch_coop_mixed(int dir, int warps, const SweepArgs& a, const Phys& P,
+                              cudaStream_t s);
 cudaError_t launch_ycell(const SweepArgs& a, const Phys& P, cudaStream_t s);
 cudaError_t launch_xcell_mixed(const SweepArgs& a, const Phys& P, cudaStream_t s);
+// The FMA FP64 stage set (hb_fast.cu): kernel = HB_KERNEL_* (include/hydro_b200.h).
+cudaError_t launch_sweep_fast(int dir, int kernel, const SweepArgs& a, const Phys& P,
+                              cudaStream_t s);
+int sweep_fast_blocks_per_sm(int dir);
+cudaError_t launch_courant_fast(const double* u, int nx, int ny, int nxt, long long vs,
+                                const Phys& P, unsigned long long* cour, cudaStream_t s);
 // The mixed-precision sweep (hb_mixed.cu).
 cudaError_t launch_sweep_mixed(int dir, const SweepArgs& a, const Phys& P, cudaStream_t s);
 int sweep_mixed_blocks_per_sm(int dir);

@@ -243,7 +243,8 @@ __device__ __forceinline__ void march(const SweepArgs& a, const typename S::Cons
 template <int DIR, class S>
 __device__ __forceinline__ void sweep_body(const SweepArgs& a, const Phys& P) {
     const int l = blockIdx.x * blockDim.x + threadIdx.x;
-    bool active = l < a.nlines;
+    const int segi = a.w_lo + (int)blockIdx.y;
+    bool active = l < a.nlines && segi < a.w_hi;
     double dt = a.dt;
     if (a.clk) {
         active = active && a.clk->active;
@@ -254,7 +255,7 @@ __device__ __forceinline__ void sweep_body(const SweepArgs& a, const Phys& P) {
         const typename S::Consts C = S::consts(P);
         const LineGeom<DIR> g(a, l);
         const double dtdx = dt / P.dx;
-        const int k0 = 2 + blockIdx.y * a.seg;
+        const int k0 = 2 + segi * a.seg;
         const int k1 = min(k0 + a.seg, a.n - 2);
         march<DIR, S>(a, C, g, k0, k1, dtdx, cx, cy);
     }
@@ -427,9 +428,9 @@ __device__ __forceinline__ void xcell_window(const SweepArgs& a, const typename 
 // Grid: x = rows, y = ceil(windows / warps per CTA).
 template <class S>
 __device__ __forceinline__ void xcell_body(const SweepArgs& a, const Phys& P) {
-    const int win = blockIdx.y * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int win = a.w_lo + blockIdx.y * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int row = blockIdx.x;
-    bool active = row < a.nlines;
+    bool active = row < a.nlines && win < a.w_hi;
     double dt = a.dt;
     if (a.clk) {
         active = active && a.clk->active;

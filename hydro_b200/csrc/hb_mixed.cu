@@ -3,6 +3,7 @@
 // division / square root and FMA contraction (see the Makefile).
 #include "hb_kernels.cuh"
 #include "hb_march.cuh"
+#include "hb_coop.cuh"
 #include "hb_stages_mixed.cuh"
 #include "hb_batch_body.cuh"
 
@@ -20,16 +21,45 @@ xcell_mixed_kernel(const SweepArgs a, const Phys P) {
 }
 
 cudaError_t launch_xcell_mixed(const SweepArgs& a, const Phys& P, cudaStream_t s) {
-    const int nwin = (a.n - 2 + window_out<MixedStages>() - 1) / window_out<MixedStages>();
+    const int nwin =
+        window_span(a, (a.n - 2 + window_out<MixedStages>() - 1) / window_out<MixedStages>());
     const int wpc = kCellThreads / 32;
+    if (nwin == 0) return cudaSuccess;
     dim3 grid(a.nlines, (nwin + wpc - 1) / wpc);
     xcell_mixed_kernel<<<grid, kCellThreads, 0, s>>>(a, P);
     return cudaGetLastError();
 }
 
+// The cooperative window (hb_coop.cuh) with the mixed stage set, at the warp
+// window's thread count per SM (kMixedCellMinBlocks CTAs of 64 threads).
+template <int DIR, int G>
+__global__ void __launch_bounds__(32 * G, kMixedCellMinBlocks * 2 / G)
+coop_mixed_kernel(const SweepArgs a, const Phys P) {
+    coop_body<MixedStages, DIR, G>(a, P);
+}
+
+template <int G>
+static cudaError_t launch_coop_mixed_g(int dir, const SweepArgs& a, const Phys& P,
+                                       cudaStream_t s) {
+    const int nwin = window_span(a, coop_windows<G>(a.n));
+    if (nwin == 0) return cudaSuccess;
+    const dim3 grid(a.nlines, nwin);
+    if (dir == 1) coop_mixed_kernel<1, G><<<grid, 32 * G, 0, s>>>(a, P);
+    else coop_mixed_kernel<2, G><<<grid, 32 * G, 0, s>>>(a, P);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_coop_mixed(int dir, int warps, const SweepArgs& a, const Phys& P,
+                              cudaStream_t s) {
+    if (warps == 8) return launch_coop_mixed_g<8>(dir, a, P, s);
+    return launch_coop_mixed_g<4>(dir, a, P, s);
+}
+
 cudaError_t launch_sweep_mixed(int dir, const SweepArgs& a, const Phys& P, cudaStream_t s) {
     const int nl = a.n - 4;
-    dim3 grid((a.nlines + kSweepThreads - 1) / kSweepThreads, (nl + a.seg - 1) / a.seg);
+    const int nseg = window_span(a, (nl + a.seg - 1) / a.seg);
+    if (nseg == 0) return cudaSuccess;
+    dim3 grid((a.nlines + kSweepThreads - 1) / kSweepThreads, nseg);
     if (dir == 1)
         sweep_mixed_kernel<1><<<grid, kSweepThreads, 0, s>>>(a, P);
     else

@@ -97,6 +97,8 @@ hb::SweepArgs args_for(const hydroparam_t* H, int dir, const double* in, double*
         a.n = a.nyt;
     }
     a.seg = 0;  // the cell-per-lane kernels take no segment length
+    a.w_lo = 0;
+    a.w_hi = hb::kWholeLine;
     return a;
 }
 

@@ -88,11 +88,11 @@ struct hb_domain {
     int bnd_left = 1, bnd_right = 1, bnd_down = 1, bnd_up = 1;
     int sm_count = 0;  // cudaDevAttrMultiProcessorCount, read in domain_alloc
     int precision = HB_PREC_FP64;
-    int xsweep[2] = {HB_XSWEEP_CELL, HB_XSWEEP_CELL};  // x-sweep kernel per precision
-    int seg[2][3] = {{0, 64, 64}, {0, 64, 64}};  // [precision][direction] segment lengths
-    // FP64 y sweep one cell per lane (grids of at most kYcellMaxCells cells)
-    // instead of marching segments.
-    bool ycell = false;
+    // Sweep kernel (HB_KERNEL_*) per [precision][direction]; set in domain_alloc.
+    int kern[3][3] = {{0, HB_KERNEL_WARP, HB_KERNEL_MARCH},
+                      {0, HB_KERNEL_WARP, HB_KERNEL_MARCH},
+                      {0, HB_KERNEL_WARP, HB_KERNEL_MARCH}};
+    int seg[3][3] = {{0, 64, 64}, {0, 64, 64}, {0, 64, 64}};  // [precision][direction]
     bool cour_valid = false;  // cour holds the maxima of the current state
     int h_nstep = 0;          // host view of the clock's nstep (parity of launches)
     long long launches = 0;
@@ -204,6 +204,27 @@ static int choose_seg(int nlines, int nl, int slots, int cap) {
     return best < cap ? best : cap;
 }
 
+// The measured default sweep kernel of a grid (per-launch times on B200,
+// centred blast; FP64 and FMA FP64 alike).
+//  - x, FP64: the 4-warp cooperative window from 2^20 cells (4096^2: 0.821
+//    against 0.858 ms for the warp window; 1024^2: 0.069 against 0.072 ms),
+//    the warp window below (256^2: 0.017 against 0.020 ms).
+//  - x, mixed: the warp window with two cells per lane (4096^2: 0.419 ms; the
+//    cooperative window one cell per thread: 0.518 ms).
+//  - y, FP64: the warp window along columns up to kYcellMaxCells cells
+//    (against marching segments: 256^2 0.017 against 0.074 ms, 1024^2 0.076
+//    against 0.101 ms, 2048^2 0.253 against 0.256 ms), the marcher above
+//    (4096^2: 0.811 against 0.920 ms; the cooperative window 0.977 ms).
+//  - y, mixed: the marcher, which its batched y items share, so that their
+//    results stay equal.
+static int default_kernel(const hb_domain* d, int prec, int dir) {
+    const long long cells = (long long)d->nx * d->ny;
+    if (dir == 1)
+        return (prec != HB_PREC_MIXED && cells >= (1ll << 20)) ? HB_KERNEL_COOP : HB_KERNEL_WARP;
+    if (prec != HB_PREC_MIXED && cells <= kYcellMaxCells) return HB_KERNEL_WARP;
+    return HB_KERNEL_MARCH;
+}
+
 static int domain_alloc(hb_domain* d) {
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
@@ -211,21 +232,18 @@ static int domain_alloc(hb_domain* d) {
     HB_CU(cudaGetDevice(&d->device));
     HB_CU(cudaDeviceGetAttribute(&d->sm_count, cudaDevAttrMultiProcessorCount, d->device));
     for (int dir = 1; dir <= 2; dir++) {
-        for (int prec = 0; prec < 2; prec++) {
-            const int per_sm = prec == HB_PREC_FP64
-                                   ? hb::sweep_blocks_per_sm(dir, d->P.unit_slope != 0)
-                                   : hb::sweep_mixed_blocks_per_sm(dir);
+        for (int prec = 0; prec < 3; prec++) {
+            const int per_sm = prec == HB_PREC_FP64    ? hb::sweep_blocks_per_sm(dir, d->P.unit_slope != 0)
+                               : prec == HB_PREC_MIXED ? hb::sweep_mixed_blocks_per_sm(dir)
+                                                       : hb::sweep_fast_blocks_per_sm(dir);
             const int slots = d->sm_count * per_sm;
-            const int cap = (prec == HB_PREC_FP64 && dir == 2) ? 32 : 1 << 30;
+            const int cap = (prec != HB_PREC_MIXED && dir == 2) ? 32 : 1 << 30;
             d->seg[prec][dir] = dir == 1 ? choose_seg(d->ny, d->nx, slots, cap)
                                          : choose_seg(d->nx, d->ny, slots, cap);
         }
     }
-    // The y sweep one cell per lane beats marching segments up to about
-    // 2048^2 (measured: 250x125 4.7x, 512^2 2.1x, 1024^2 1.2x, 2048^2 1.06x
-    // faster; 4096^2 0.7% slower).  FP64 only: the mixed set keeps the marcher,
-    // which its batched y items share, so that their results stay equal.
-    d->ycell = (long long)d->nx * d->ny <= kYcellMaxCells;
+    for (int prec = 0; prec < 3; prec++)
+        for (int dir = 1; dir <= 2; dir++) d->kern[prec][dir] = default_kernel(d, prec, dir);
     HB_CU(cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking));
     HB_CU(cudaMalloc(&d->A, d->nelem * sizeof(double)));
     HB_CU(cudaMalloc(&d->B, d->nelem * sizeof(double)));
@@ -306,6 +324,8 @@ static SweepArgs sweep_args(hb_domain* d, int dir, const double* in, double* out
         a.n = d->nyt;
     }
     a.seg = d->seg[d->precision][dir];
+    a.w_lo = 0;
+    a.w_hi = hb::kWholeLine;
     return a;
 }
 
@@ -327,15 +347,24 @@ static int launch_sweep_timed(hb_domain* d, int dir, const SweepArgs& a) {
         e1 = take_event(d);
         HB_CU(cudaEventRecord(e0, d->stream));
     }
-    const bool cell = dir == 1 && d->xsweep[d->precision] == HB_XSWEEP_CELL;
-    if (d->precision == HB_PREC_MIXED) {
-        HB_CU(cell ? hb::launch_xcell_mixed(a, d->P, d->stream)
-                   : hb::launch_sweep_mixed(dir, a, d->P, d->stream));
-    } else if (dir == 2 && d->ycell) {
-        HB_CU(hb::launch_ycell(a, d->P, d->stream));
+    const int kern = d->kern[d->precision][dir];
+    if (d->precision == HB_PREC_FP64_FMA) {
+        HB_CU(hb::launch_sweep_fast(dir, kern, a, d->P, d->stream));
+    } else if (d->precision == HB_PREC_MIXED) {
+        if (kern == HB_KERNEL_COOP || kern == HB_KERNEL_COOP8)
+            HB_CU(hb::launch_coop_mixed(dir, kern == HB_KERNEL_COOP8 ? 8 : 4, a, d->P, d->stream));
+        else if (kern == HB_KERNEL_WARP && dir == 1)
+            HB_CU(hb::launch_xcell_mixed(a, d->P, d->stream));
+        else
+            HB_CU(hb::launch_sweep_mixed(dir, a, d->P, d->stream));
     } else {
-        HB_CU(cell ? hb::launch_xcell(a, d->P, d->stream)
-                   : hb::launch_sweep(dir, a, d->P, d->stream));
+        if (kern == HB_KERNEL_COOP || kern == HB_KERNEL_COOP8)
+            HB_CU(hb::launch_coop(dir, kern == HB_KERNEL_COOP8 ? 8 : 4, a, d->P, d->stream));
+        else if (kern == HB_KERNEL_WARP)
+            HB_CU(dir == 1 ? hb::launch_xcell(a, d->P, d->stream)
+                           : hb::launch_ycell(a, d->P, d->stream));
+        else
+            HB_CU(hb::launch_sweep(dir, a, d->P, d->stream));
     }
     d->launches += 1;
     if (d->prof) {
@@ -389,6 +418,62 @@ extern "C" int hydro_b200_domain_sweep(hb_domain* d, int stage, int idim, double
     const int rc = launch_sweep_timed(d, idim, a);
     if (rc) return rc;
     d->cour_valid = stage == 1 && fuse_courant;
+    return HB_OK;
+}
+
+// Window (segment) geometry of the domain's sweep kernel in direction dir:
+// `total` windows per line, of which [lo, hi) read no ghost cell.  Window w
+// of the cell-window kernels outputs [W w, W w + W) and reads two cells more
+// on each side; segment w of the marching kernels outputs
+// [2 + seg w, 2 + seg (w + 1)) and reads the same margins.
+static void window_bounds(const hb_domain* d, int dir, int* total, int* lo, int* hi) {
+    const int n = dir == 1 ? d->nxt : d->nyt;
+    const int kern = d->kern[d->precision][dir];
+    if (kern == HB_KERNEL_MARCH) {
+        const int seg = d->seg[d->precision][dir];
+        *total = (n - 4 + seg - 1) / seg;
+        *lo = 1;
+        *hi = (n - 6) / seg;
+    } else {
+        int W = hb::kCellWarpOut;
+        if (kern == HB_KERNEL_COOP) W = 32 * 4 - 4;
+        if (kern == HB_KERNEL_COOP8) W = 32 * 8 - 4;
+        if (kern == HB_KERNEL_WARP && dir == 1 && d->precision == HB_PREC_MIXED)
+            W = hb::kCellWarpOut2;
+        *total = (n - 2 + W - 1) / W;
+        *lo = 1;
+        *hi = (n - 4) / W;
+    }
+    if (*hi > *total) *hi = *total;
+    if (*hi < *lo) *hi = *lo;  // no ghost-free window: part 1 is empty
+}
+
+// One part of a sweep (see include/hydro_b200.h): part 1 the ghost-free
+// windows, part 2 the others, part 0 all of them.
+extern "C" int hydro_b200_domain_sweep_part(hb_domain* d, int stage, int idim, double dt,
+                                            int fuse_courant, int part) {
+    if (!d) return set_error(HB_ERR_ARG, "null domain");
+    if (part == 0) return hydro_b200_domain_sweep(d, stage, idim, dt, fuse_courant);
+    if (idim != 1 && idim != 2) return set_error(HB_ERR_ARG, "idim=%d: expected 1 or 2", idim);
+    if (stage != 0 && stage != 1) return set_error(HB_ERR_ARG, "stage=%d: expected 0 or 1", stage);
+    if (part != 1 && part != 2) return set_error(HB_ERR_ARG, "part=%d: expected 0, 1 or 2", part);
+    if (stage == 0 && fuse_courant)
+        return set_error(HB_ERR_ARG, "the Courant reduction fuses into the second sweep only");
+    if (fuse_courant && part == 1) HB_CU(cudaMemsetAsync(d->cour, 0, kCourBytes, d->stream));
+    SweepArgs a = stage == 0 ? sweep_args(d, idim, d->A, d->B, nullptr, dt, nullptr)
+                             : sweep_args(d, idim, d->B, d->A, nullptr, dt,
+                                          fuse_courant ? d->cour : nullptr);
+    int total, lo, hi;
+    window_bounds(d, idim, &total, &lo, &hi);
+    const int ranges[2][2] = {{part == 1 ? lo : 0, part == 1 ? hi : lo}, {hi, total}};
+    for (int r = 0; r < (part == 1 ? 1 : 2); r++) {
+        if (ranges[r][1] <= ranges[r][0]) continue;
+        a.w_lo = ranges[r][0];
+        a.w_hi = ranges[r][1];
+        const int rc = launch_sweep_timed(d, idim, a);
+        if (rc) return rc;
+    }
+    d->cour_valid = stage == 1 && fuse_courant && part == 2;
     return HB_OK;
 }
 
@@ -453,8 +538,9 @@ extern "C" int hydro_b200_domain_vtk_base64(hb_domain* d, int var, char* host_ou
 
 extern "C" int hydro_b200_domain_set_precision(hb_domain* d, int precision) {
     if (!d) return set_error(HB_ERR_ARG, "null domain");
-    if (precision != HB_PREC_FP64 && precision != HB_PREC_MIXED)
-        return set_error(HB_ERR_ARG, "precision=%d: expected HB_PREC_FP64 or HB_PREC_MIXED",
+    if (precision != HB_PREC_FP64 && precision != HB_PREC_MIXED && precision != HB_PREC_FP64_FMA)
+        return set_error(HB_ERR_ARG,
+                         "precision=%d: expected HB_PREC_FP64, HB_PREC_MIXED or HB_PREC_FP64_FMA",
                          precision);
     d->precision = precision;
     return HB_OK;
@@ -462,11 +548,33 @@ extern "C" int hydro_b200_domain_set_precision(hb_domain* d, int precision) {
 
 extern "C" int hydro_b200_domain_set_xsweep(hb_domain* d, int precision, int mode) {
     if (!d) return set_error(HB_ERR_ARG, "null domain");
-    if ((precision != HB_PREC_FP64 && precision != HB_PREC_MIXED) ||
+    if (precision < HB_PREC_FP64 || precision > HB_PREC_FP64_FMA ||
         (mode != HB_XSWEEP_MARCH && mode != HB_XSWEEP_CELL))
         return set_error(HB_ERR_ARG, "precision=%d mode=%d: invalid", precision, mode);
-    d->xsweep[precision] = mode;
+    d->kern[precision][1] = mode == HB_XSWEEP_CELL ? HB_KERNEL_WARP : HB_KERNEL_MARCH;
     return HB_OK;
+}
+
+extern "C" int hydro_b200_domain_set_kernel(hb_domain* d, int precision, int idim, int kernel) {
+    if (!d) return set_error(HB_ERR_ARG, "null domain");
+    if (precision < HB_PREC_FP64 || precision > HB_PREC_FP64_FMA || (idim != 1 && idim != 2))
+        return set_error(HB_ERR_ARG, "precision=%d idim=%d: invalid", precision, idim);
+    if (kernel == HB_KERNEL_AUTO) kernel = default_kernel(d, precision, idim);
+    const bool known = kernel == HB_KERNEL_MARCH || kernel == HB_KERNEL_WARP ||
+                       kernel == HB_KERNEL_COOP || kernel == HB_KERNEL_COOP8;
+    // The mixed set has no warp window along columns.
+    if (!known || (precision == HB_PREC_MIXED && idim == 2 && kernel == HB_KERNEL_WARP))
+        return set_error(HB_ERR_ARG, "kernel=%d: not available for precision %d, idim %d", kernel,
+                         precision, idim);
+    d->kern[precision][idim] = kernel;
+    return HB_OK;
+}
+
+extern "C" int hydro_b200_domain_get_kernel(hb_domain* d, int precision, int idim) {
+    if (!d || precision < HB_PREC_FP64 || precision > HB_PREC_FP64_FMA ||
+        (idim != 1 && idim != 2))
+        return set_error(HB_ERR_ARG, "invalid domain, precision or idim"), -1;
+    return d->kern[precision][idim];
 }
 
 extern "C" int hydro_b200_domain_profile(hb_domain* d, int enable) {
@@ -520,7 +628,10 @@ static int ensure_courant(hb_domain* d) {
     if (d->cour_valid) return HB_OK;
     HB_CU(cudaMemsetAsync(d->cour, 0, kCourBytes, d->stream));
     // The per-cell formula of the domain's precision, as in the fused reduction.
-    if (d->precision == HB_PREC_MIXED) {
+    if (d->precision == HB_PREC_FP64_FMA) {
+        HB_CU(hb::launch_courant_fast(d->A, d->nx, d->ny, d->nxt, d->vs, d->P, d->cour,
+                                      d->stream));
+    } else if (d->precision == HB_PREC_MIXED) {
         HB_CU(hb::launch_courant_mixed(d->A, d->nx, d->ny, d->nxt, d->vs, d->P, d->cour,
                                        d->stream));
     } else {
@@ -587,13 +698,14 @@ static std::vector<unsigned char> pair_key(const hb_domain* d) {
     struct Key {
         Phys P;
         double courant_factor;
-        int precision, xsweep, seg1, seg2, bnd[4];
+        int precision, kern1, kern2, seg1, seg2, bnd[4];
     } k;
     memset(&k, 0, sizeof(k));
     k.P = d->P;
     k.courant_factor = d->courant_factor;
     k.precision = d->precision;
-    k.xsweep = d->xsweep[d->precision];
+    k.kern1 = d->kern[d->precision][1];
+    k.kern2 = d->kern[d->precision][2];
     k.seg1 = d->seg[d->precision][1];
     k.seg2 = d->seg[d->precision][2];
     k.bnd[0] = d->bnd_left;
@@ -704,6 +816,12 @@ extern "C" int hydro_b200_domain_get_clock(hb_domain* d, double* t, int* nstep, 
     return HB_OK;
 }
 
+extern "C" int hydro_b200_domain_reserve_dts(hb_domain* d, int n) {
+    if (!d) return set_error(HB_ERR_ARG, "null domain");
+    if (n < 0) return set_error(HB_ERR_ARG, "n=%d: expected >= 0", n);
+    return ensure_dts(d, n);
+}
+
 extern "C" int hydro_b200_domain_get_dts(hb_domain* d, double* dts, int n) {
     if (!d || !dts) return set_error(HB_ERR_ARG, "null argument");
     if (n > d->ndts) return set_error(HB_ERR_ARG, "only %d dt records reserved", d->ndts);
@@ -748,9 +866,10 @@ static hb_domain* mirror_for(const hydroparam_t* H, hydrovar_t* Hv) {
     if (!d) return nullptr;
     const char* prec = getenv("HYDRO_B200_PRECISION");
     if (prec && strcmp(prec, "mixed") == 0) d->precision = HB_PREC_MIXED;
+    if (prec && strcmp(prec, "fma") == 0) d->precision = HB_PREC_FP64_FMA;
     const char* xs = getenv("HYDRO_B200_XSWEEP");
-    if (xs && strcmp(xs, "cell") == 0) d->xsweep[0] = d->xsweep[1] = HB_XSWEEP_CELL;
-    if (xs && strcmp(xs, "march") == 0) d->xsweep[0] = d->xsweep[1] = HB_XSWEEP_MARCH;
+    if (xs && strcmp(xs, "cell") == 0) d->kern[0][1] = d->kern[1][1] = HB_KERNEL_WARP;
+    if (xs && strcmp(xs, "march") == 0) d->kern[0][1] = d->kern[1][1] = HB_KERNEL_MARCH;
     if (hydro_b200_domain_upload(d, Hv->uold) != HB_OK) {
         hydro_b200_domain_destroy(d);
         return nullptr;

@@ -52,11 +52,24 @@ __device__ __forceinline__ double omax(double x, double y) { return x > y ? x : 
 __device__ __forceinline__ double cfmax(double x, double y) { return x >= y ? x : y; }
 __device__ __forceinline__ double cfmin(double x, double y) { return x <= y ? x : y; }
 
+// a / b, IEEE-rounded, for a denominator b that is finite and nonzero (every
+// call site divides by a positive quantity of a valid state).  A zero
+// numerator gives its signed zero as the product a * b, which has the
+// quotient's sign and value, without entering the division: the IEEE division
+// sequence sends a zero numerator down its slow path (a called subroutine),
+// and a cell at rest (zero velocities, uniform pressure) meets 14 such
+// numerators per sweep.  Nonzero numerators take the ordinary division, so
+// the result is bitwise a / b in every case.
+__device__ __forceinline__ double zdiv(double a, double b) {
+    if (a == 0.0) return a * b;
+    return a / b;
+}
+
 // constoprim.c:37-52 then equation_of_state.c:41-48.
 __device__ __forceinline__ void cons_to_prim(const Phys& P, const Cons& u, Prim& q, double& c) {
     double r = omax(u.d, P.smallr);
-    double un = u.mn / r;
-    double ut = u.mt / r;
+    double un = zdiv(u.mn, r);
+    double ut = zdiv(u.mt, r);
     double eken = 0.5 * ((un * un) + (ut * ut));
     double e = u.e / r - eken;
     double base = P.gm1 * r * e;
@@ -128,10 +141,10 @@ __device__ __forceinline__ void trace1(const TraceK& K, const Prim& q, const Pri
     double csq = cc * cc;
     double rOcc = q.r / cc;
     double OrOcc = cc / q.r;
-    double dprcc = dq.p / (q.r * cc);
+    double dprcc = zdiv(dq.p, q.r * cc);
     double alpham = 0.5 * (dprcc - dq.u) * rOcc;
     double alphap = 0.5 * (dprcc + dq.u) * rOcc;
-    double alpha0r = dq.r - dq.p / csq;
+    double alpha0r = dq.r - zdiv(dq.p, csq);
     double alpha0v = dq.v;
     double upcc = q.u + cc;
     double umcc = q.u - cc;
@@ -188,25 +201,25 @@ __device__ __forceinline__ Cons riemann_flux(const Phys& P, const Prim& ql, cons
 
     for (int iter = 0; iter < P.niter; iter++) {
         double pst = pstar;
-        double wwl = sqrt(cl * (1.0 + gamma6 * (pst - pl) / pl));
-        double wwr = sqrt(cr * (1.0 + gamma6 * (pst - pr) / pr));
+        double wwl = sqrt(cl * (1.0 + zdiv(gamma6 * (pst - pl), pl)));
+        double wwr = sqrt(cr * (1.0 + zdiv(gamma6 * (pst - pr), pr)));
         double swwl = wwl * wwl;
         double qlw = 2.0 * wwl * swwl / (swwl + cl);
         double qrw = 2.0 * wwr * (wwr * wwr) / ((wwr * wwr) + cr);
-        double usl = ul - (pst - pl) / wwl;
-        double usr = ur + (pst - pr) / wwr;
+        double usl = ul - zdiv(pst - pl, wwl);
+        double usr = ur + zdiv(pst - pr, wwr);
         double tmp = (qrw * qlw / (qrw + qlw) * (usl - usr));
         double delp = omax(tmp, (-pst));
         pst += delp;
-        double tmp2 = delp / (pst + P.smallpp);
+        double tmp2 = zdiv(delp, pst + P.smallpp);
         double conv = fabs(tmp2);
         pstar = pst;
         if (!(conv > 1e-6)) break;
     }
 
-    wr = sqrt(cr * (1.0 + gamma6 * (pstar - pr) / pr));
-    wl = sqrt(cl * (1.0 + gamma6 * (pstar - pl) / pl));
-    double ustar = 0.5 * (ul + (pl - pstar) / wl + ur - (pr - pstar) / wr);
+    wr = sqrt(cr * (1.0 + zdiv(gamma6 * (pstar - pr), pr)));
+    wl = sqrt(cl * (1.0 + zdiv(gamma6 * (pstar - pl), pl)));
+    double ustar = 0.5 * (ul + zdiv(pl - pstar, wl) + ur - zdiv(pr - pstar, wr));
     bool left = ustar > 0.0;
     double sgnm = left ? 1.0 : -1.0;
     double ro = left ? rl : rr;
@@ -215,7 +228,7 @@ __device__ __forceinline__ Cons riemann_flux(const Phys& P, const Prim& ql, cons
     double wo = left ? wl : wr;
     double co = sqrt(fabs(gamma * po / ro));
     co = cfmax(smallc, co);
-    double rstar = ro / (1.0 + ro * (po - pstar) / (wo * wo));
+    double rstar = ro / (1.0 + zdiv(ro * (po - pstar), wo * wo));
     rstar = cfmax(rstar, smallr);
     double cstar = sqrt(fabs(gamma * pstar / rstar));
     cstar = cfmax(smallc, cstar);

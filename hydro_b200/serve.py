@@ -126,9 +126,21 @@ class BatchBackend:
         self.batch.close()
 
 
+# Side buckets of the latency breakdown: (label, lowest side, highest side).
+SIDE_BUCKETS = (("side<=256", 0, 256), ("256<side<=1024", 257, 1024), ("side>1024", 1025, 1 << 30))
+
+
+def _pct(x, q):
+    return round(float(np.percentile(x, q)), 4) if len(x) else None
+
+
 @dataclass
 class ServeStats:
     completed: list = field(default_factory=list)   # (rid, latency s, steps, cells)
+    # Requests still queued or running when the loop stopped: (rid, age s at
+    # the cutoff, "queued" | "running", cells).  Their time to solution is
+    # unknown but at least their age.
+    censored: list = field(default_factory=list)
     admitted: int = 0
     arrived: int = 0
     wall_s: float = 0.0
@@ -141,14 +153,39 @@ class ServeStats:
 
     def summary(self) -> dict:
         lat = np.array([c[1] for c in self.completed]) if self.completed else np.zeros(0)
+        ages = np.array([c[1] for c in self.censored]) if self.censored else np.zeros(0)
         q = [s[1] for s in self.queue_samples]
+        # Every request that arrived and was not rejected: completed ones at
+        # their time to solution, censored ones at their age.  Percentiles of
+        # this set are lower bounds on the true percentiles of the stream.
+        both = np.concatenate([lat, ages])
+        by_side = {}
+        for label, lo, hi in SIDE_BUCKETS:
+            cl = [c[1] for c in self.completed if lo <= math.isqrt(c[3]) <= hi]
+            ce = [c[1] for c in self.censored if lo <= math.isqrt(c[3]) <= hi]
+            by_side[label] = {"completed": len(cl), "p50_s": _pct(cl, 50), "p99_s": _pct(cl, 99),
+                              "censored": len(ce),
+                              "censored_age_max_s": round(max(ce), 4) if ce else None,
+                              "p50_lower_bound_s": _pct(cl + ce, 50),
+                              "p99_lower_bound_s": _pct(cl + ce, 99)}
         return {
             "arrived": self.arrived, "admitted": self.admitted,
             "completed": len(self.completed),
             "wall_s": round(self.wall_s, 3),
             "mcell_updates_per_s": round(self.cell_steps / max(self.wall_s, 1e-9) / 1e6, 3),
-            "p50_s": round(float(np.percentile(lat, 50)), 4) if lat.size else None,
-            "p99_s": round(float(np.percentile(lat, 99)), 4) if lat.size else None,
+            "p50_s": _pct(lat, 50),
+            "p99_s": _pct(lat, 99),
+            "latency_note": "p50_s/p99_s cover completed requests only; *_lower_bound_s also "
+                            "count every censored request (queued or running at the cutoff) "
+                            "at its age, a lower bound on its time to solution",
+            "censored": {"count": len(self.censored),
+                         "queued": sum(1 for c in self.censored if c[2] == "queued"),
+                         "running": sum(1 for c in self.censored if c[2] == "running"),
+                         "age_p50_s": _pct(ages, 50), "age_p99_s": _pct(ages, 99),
+                         "age_max_s": round(float(ages.max()), 4) if ages.size else None},
+            "p50_lower_bound_s": _pct(both, 50),
+            "p99_lower_bound_s": _pct(both, 99),
+            "by_side": by_side,
             "queue_max": max(q) if q else 0,
             "queue_end": q[-1] if q else 0,
             "running_end": self.unfinished,
@@ -258,8 +295,18 @@ class Server:
             if dtc > 0:
                 k = int(max(1, min(self.max_chunk, round(k * self.chunk_target_s / dtc))))
         st.wall_s = self.clock() - t0
-        arrived_waiting = len(waiting) + sum(1 for r in pending if r.arrival <= st.wall_s)
-        st.arrived += sum(1 for r in pending if r.arrival <= st.wall_s)
+        late = [r for r in pending if r.arrival <= st.wall_s]  # arrived, never looked at
+        arrived_waiting = len(waiting) + len(late)
+        st.arrived += len(late)
         st.queue_samples.append((st.wall_s, arrived_waiting, len(running)))
         st.unfinished = len(running)
+        # Censored requests: their age at the cutoff bounds their time to
+        # solution.  Arrivals not yet looked at get the arrival rule (rejected
+        # when larger than the whole budget).
+        fit = [r for r in late if self.backend.can_ever_fit(r)]
+        st.rejected += len(late) - len(fit)
+        for req in [w[0] for w in waiting] + fit:
+            st.censored.append((req.rid, st.wall_s - req.arrival, "queued", req.cells))
+        for req, _ in running.values():
+            st.censored.append((req.rid, st.wall_s - req.arrival, "running", req.cells))
         return st

@@ -120,7 +120,8 @@ class HydroRun:
 class Domain:
     """Device-resident state (hb_domain)."""
 
-    def __init__(self, H: HydroParam, precision: str = "fp64", xsweep: str | None = None):
+    def __init__(self, H: HydroParam, precision: str = "fp64", xsweep: str | None = None,
+                 kernels: tuple | None = None):
         self.lib = load()
         self.H = H
         self.h = self.lib.hydro_b200_domain_create(C.byref(H))
@@ -132,8 +133,23 @@ class Domain:
         if xsweep is not None:
             check(self.lib.hydro_b200_domain_set_xsweep(self.h, _lib.PRECISIONS[precision],
                                                         _lib.XSWEEPS[xsweep]))
+        if kernels is not None:
+            self.set_kernels(*kernels)
         self.shape = state_shape(H)
         self.nbytes = int(np.prod(self.shape)) * 8
+
+    def set_kernels(self, x: str | None = None, y: str | None = None) -> None:
+        """Sweep kernels of this domain's precision: "march", "warp", "coop",
+        "coop8" or "auto" per direction (None keeps the current one)."""
+        prec = _lib.PRECISIONS[self.precision]
+        for idim, k in ((1, x), (2, y)):
+            if k is not None:
+                check(self.lib.hydro_b200_domain_set_kernel(self.h, prec, idim, _lib.KERNELS[k]))
+
+    def kernels(self) -> tuple:
+        names = {v: k for k, v in _lib.KERNELS.items()}
+        prec = _lib.PRECISIONS[self.precision]
+        return tuple(names[self.lib.hydro_b200_domain_get_kernel(self.h, prec, i)] for i in (1, 2))
 
     @property
     def state_ptr(self) -> int:
@@ -177,8 +193,12 @@ class Domain:
         return cx.value, cy.value
 
     # --- one sweep at a time, and halo strips (domain split) ------------------
-    def sweep(self, stage: int, idim: int, dt: float, fuse_courant: bool = False) -> None:
-        check(self.lib.hydro_b200_domain_sweep(self.h, stage, idim, dt, int(fuse_courant)))
+    def sweep(self, stage: int, idim: int, dt: float, fuse_courant: bool = False,
+              part: int = 0) -> None:
+        """One sweep of a step (stage 0: first, 1: second); part 1 / 2 sweep
+        the ghost-free windows / the others (0: all)."""
+        check(self.lib.hydro_b200_domain_sweep_part(self.h, stage, idim, dt, int(fuse_courant),
+                                                    part))
 
     def halo_count(self, idim: int) -> int:
         return int(self.lib.hydro_b200_domain_halo_count(self.h, idim))
@@ -206,6 +226,10 @@ class Domain:
         t, n, dt = C.c_double(), C.c_int(), C.c_double()
         check(self.lib.hydro_b200_domain_get_clock(self.h, C.byref(t), C.byref(n), C.byref(dt)))
         return t.value, n.value, dt.value
+
+    def reserve_dts(self, n: int) -> None:
+        """Record the dt of up to n steps from the next set_clock on."""
+        check(self.lib.hydro_b200_domain_reserve_dts(self.h, n))
 
     def get_dts(self, n: int) -> np.ndarray:
         """dt of steps 0 .. n-1 of the launch-only driver (device record)."""

@@ -173,7 +173,7 @@ def compute_dt(courant_factor: float, dx: float, smallc: float, cx: float, cy: f
 class GpuSubdomain:
     """A subdomain held by the library (hb_domain) with device halo buffers."""
 
-    def __init__(self, H, box: Box, rank: int, device, precision: str = "fp64"):
+    def __init__(self, H, box: Box, rank: int, device, precision: str = "fp64", kernels=None):
         import torch
 
         from .solver import Domain
@@ -181,7 +181,8 @@ class GpuSubdomain:
         self.H, self.box, self.rank = H, box, rank
         self.device = torch.device(device)
         with torch.cuda.device(self.device):
-            self.dom = Domain(H, precision=precision)
+            self.dom = Domain(H, precision=precision, kernels=kernels)
+            self.comm_stream = None  # DistComm's transfer stream (created on first use)
             self.stream = torch.cuda.ExternalStream(self.dom.stream_ptr, device=self.device)
             self.send = {}
             self.recv = {}
@@ -203,8 +204,8 @@ class GpuSubdomain:
     def courant(self):
         return self.dom.courant()
 
-    def sweep(self, stage: int, idim: int, dt: float, fuse: bool) -> None:
-        self.dom.sweep(stage, idim, dt, fuse)
+    def sweep(self, stage: int, idim: int, dt: float, fuse: bool, part: int = 0) -> None:
+        self.dom.sweep(stage, idim, dt, fuse, part)
 
     def pack(self, stage: int, idim: int, side: int) -> None:
         self.dom.halo_pack(stage, idim, side, self.send[idim, side].data_ptr())
@@ -234,26 +235,56 @@ class DistComm:
         self.dist = dist
         self.group = group
 
-    def exchange(self, subs: list, idim: int) -> None:
-        import torch
-
-        (sub,) = subs
+    def _ops(self, sub, idim: int) -> list:
         ops = []
         for side in (0, 1):
             nb = sub.box.neighbour(idim, side)
             if nb >= 0:
                 ops.append(self.dist.P2POp(self.dist.isend, sub.send[idim, side], nb, self.group))
                 ops.append(self.dist.P2POp(self.dist.irecv, sub.recv[idim, side], nb, self.group))
+        return ops
+
+    def exchange(self, subs: list, idim: int) -> None:
+        self.exchange_finish(subs, self.exchange_start(subs, idim))
+
+    def exchange_start(self, subs: list, idim: int):
+        """Start the transfers of direction idim after the packs already
+        issued on the subdomain's stream.  On a GPU they run on a stream of
+        their own, so that work issued on the subdomain's stream afterwards
+        (the sweep's ghost-free windows) overlaps them."""
+        import torch
+
+        (sub,) = subs
+        ops = self._ops(sub, idim)
         if not ops:
-            return
+            return None
         stream = getattr(sub, "stream", None)
-        if stream is not None:
-            with torch.cuda.stream(stream):
-                for r in self.dist.batch_isend_irecv(ops):
-                    r.wait()
-        else:
-            for r in self.dist.batch_isend_irecv(ops):
-                r.wait()
+        if stream is None:
+            return self.dist.batch_isend_irecv(ops)
+        if getattr(sub, "comm_stream", None) is None:
+            sub.comm_stream = torch.cuda.Stream(device=sub.device)
+        packed = torch.cuda.Event()
+        packed.record(stream)
+        with torch.cuda.stream(sub.comm_stream):
+            sub.comm_stream.wait_event(packed)
+            return self.dist.batch_isend_irecv(ops)
+
+    def exchange_finish(self, subs: list, works) -> None:
+        """Order the subdomain's stream after the transfers (no host wait on a
+        GPU): work issued on it afterwards (the unpacks) sees the strips."""
+        import torch
+
+        if not works:
+            return
+        (sub,) = subs
+        stream = getattr(sub, "stream", None)
+        if stream is None:
+            for w in works:
+                w.wait()
+            return
+        with torch.cuda.stream(stream):
+            for w in works:
+                w.wait()
 
     def min(self, subs: list, x: float) -> float:
         import torch
@@ -286,6 +317,12 @@ class LocalComm:
                     s.recv[idim, side].copy_(by_rank[nb].send[idim, 1 - side])
         _sync_torch(subs)
 
+    def exchange_start(self, subs: list, idim: int):
+        return idim
+
+    def exchange_finish(self, subs: list, idim) -> None:
+        self.exchange(subs, idim)
+
     def min(self, subs: list, x: float) -> float:
         return x
 
@@ -305,12 +342,19 @@ def _sync_torch(subs) -> None:
 
 class SplitRun:
     """main.c:344-408 over subdomains.  `subs` are the subdomains this
-    process owns (one per rank with DistComm; all of them with LocalComm)."""
+    process owns (one per rank with DistComm; all of them with LocalComm).
 
-    def __init__(self, Hg, subs: list, comm):
+    With ``overlap`` each sweep is issued in two parts around its halo
+    exchange: pack the strips, start the transfers, sweep the windows that
+    read no ghost cell (hydro_b200_domain_sweep_part, part 1) while the strips
+    travel, then finish the transfers, unpack, and sweep the windows next to
+    the ghosts (part 2).  The results are the same bits as without it."""
+
+    def __init__(self, Hg, subs: list, comm, overlap: bool = False):
         self.Hg = Hg
         self.subs = subs
         self.comm = comm
+        self.overlap = overlap
         self.t = 0.0
         self.nstep = 0
         self.dt = 0.0
@@ -326,6 +370,27 @@ class SplitRun:
             for side in (0, 1):
                 if s.box.neighbour(idim, side) >= 0:
                     s.unpack(idim, side)
+
+    def _sweep_stage(self, stage: int, idim: int, fuse: bool) -> None:
+        if not self.overlap:
+            self._exchange(stage, idim)
+            for s in self.subs:
+                s.sweep(stage, idim, self.dt, fuse)
+            return
+        for s in self.subs:
+            for side in (0, 1):
+                if s.box.neighbour(idim, side) >= 0:
+                    s.pack(stage, idim, side)
+        pending = self.comm.exchange_start(self.subs, idim)
+        for s in self.subs:
+            s.sweep(stage, idim, self.dt, fuse, 1)
+        self.comm.exchange_finish(self.subs, pending)
+        for s in self.subs:
+            for side in (0, 1):
+                if s.box.neighbour(idim, side) >= 0:
+                    s.unpack(idim, side)
+        for s in self.subs:
+            s.sweep(stage, idim, self.dt, fuse, 2)
 
     def step(self) -> float:
         Hg = self.Hg
@@ -343,12 +408,8 @@ class SplitRun:
         second = 3 - first
         # The Courant maxima of the state after an odd step feed the next dt.
         fuse = self.nstep % 2 == 1
-        self._exchange(0, first)
-        for s in self.subs:
-            s.sweep(0, first, self.dt, False)
-        self._exchange(1, second)
-        for s in self.subs:
-            s.sweep(1, second, self.dt, fuse)
+        self._sweep_stage(0, first, False)
+        self._sweep_stage(1, second, fuse)
         self.dts.append(self.dt)
         self.nstep += 1
         self.t += self.dt
@@ -362,7 +423,7 @@ class SplitRun:
 
 
 def split_gpu_local(Hg, u_global: np.ndarray, nparts: int, devices=None,
-                    precision: str = "fp64"):
+                    precision: str = "fp64", overlap: bool = False, kernels=None):
     """All subdomains of an `nparts` split in this process, subdomain r on
     devices[r % len(devices)] (default: cuda:0).  Returns the SplitRun."""
     boxes = decompose(Hg.nx, Hg.ny, nparts)
@@ -370,10 +431,10 @@ def split_gpu_local(Hg, u_global: np.ndarray, nparts: int, devices=None,
     subs = []
     for r, b in enumerate(boxes):
         H = local_params(Hg, b, r, nparts)
-        s = GpuSubdomain(H, b, r, devices[r % len(devices)], precision)
+        s = GpuSubdomain(H, b, r, devices[r % len(devices)], precision, kernels)
         s.upload(scatter_state(u_global, b))
         subs.append(s)
-    return SplitRun(Hg, subs, LocalComm())
+    return SplitRun(Hg, subs, LocalComm(), overlap=overlap)
 
 
 def gather_global(Hg, subs: list, out: np.ndarray | None = None) -> np.ndarray:

@@ -210,6 +210,15 @@ int hydro_b200_domain_courant(hb_domain *d, double *cournox, double *cournoy); /
  * grid holds them.  Buffers are device pointers; all three run asynchronously
  * on the domain's stream. */
 int hydro_b200_domain_sweep(hb_domain *d, int stage, int idim, double dt, int fuse_courant);
+/* The same sweep in two parts, so that a split can overlap its halo exchange
+ * with the sweep: part 1 sweeps the windows of every line that read no ghost
+ * cell (it may run before the halos of that sweep are unpacked), part 2 the
+ * windows that do (after the unpack); part 0 is the whole sweep.  Parts 1
+ * then 2 do the work of one hydro_b200_domain_sweep, with the same results.
+ * With fuse_courant the Courant maxima are reset by part 1 and complete after
+ * part 2. */
+int hydro_b200_domain_sweep_part(hb_domain *d, int stage, int idim, double dt, int fuse_courant,
+                                 int part);
 long long hydro_b200_domain_halo_count(hb_domain *d, int idim);
 int hydro_b200_domain_halo_pack(hb_domain *d, int stage, int idim, int side, double *dst);
 int hydro_b200_domain_halo_unpack(hb_domain *d, int idim, int side, const double *src);
@@ -225,6 +234,9 @@ int hydro_b200_domain_set_clock(hb_domain *d, double t, int nstep, double dt);
 int hydro_b200_domain_launch_steps(hb_domain *d, int nsteps, int nstepmax, double tend);
 int hydro_b200_domain_get_clock(hb_domain *d, double *t, int *nstep, double *dt); /* synchronous */
 int hydro_b200_domain_get_dts(hb_domain *d, double *dts, int n); /* dt of the steps since set_clock */
+/* Reserve the device record of the dt of up to n steps; set_clock after it
+ * starts recording (hydro_b200_run reserves its own). */
+int hydro_b200_domain_reserve_dts(hb_domain *d, int n);
 /* Arithmetic of the sweeps.  HB_PREC_FP64 (default): the reference's FP64
  * operations, bit for bit.  HB_PREC_MIXED: FP32 constoprim / EOS / slope /
  * trace / Riemann sampling / flux, FP64 Newton iteration on p*, FP64 update
@@ -232,6 +244,11 @@ int hydro_b200_domain_get_dts(hb_domain *d, double *dts, int n); /* dt of the st
  * reference entry points use HB_PREC_MIXED when HYDRO_B200_PRECISION=mixed. */
 #define HB_PREC_FP64 0
 #define HB_PREC_MIXED 1
+/* HB_PREC_FP64_FMA: FP64 throughout, with FMA contraction and divisions and
+ * square roots through refined reciprocals (one per shared denominator)
+ * instead of the reference's IEEE-rounded operations in its order: within
+ * 1e-12 of the reference per cell over its 200-step 4096^2 run, not bitwise. */
+#define HB_PREC_FP64_FMA 2
 int hydro_b200_domain_set_precision(hb_domain *d, int precision);
 
 /* Kernel of the x sweep.  HB_XSWEEP_MARCH: each thread marches along a row
@@ -244,6 +261,26 @@ int hydro_b200_domain_set_precision(hb_domain *d, int precision);
 #define HB_XSWEEP_MARCH 0
 #define HB_XSWEEP_CELL 1
 int hydro_b200_domain_set_xsweep(hb_domain *d, int precision, int mode);
+
+/* Sweep kernel of one direction (idim 1: x, 2: y) and precision.  All give
+ * identical results in FP64; they differ in how lines are cut into work:
+ *   HB_KERNEL_MARCH  each thread marches along a line segment with a
+ *                    five-cell register window;
+ *   HB_KERNEL_WARP   a warp takes 32 consecutive cells of a line, one per lane
+ *                    (two per lane in the mixed x sweep), neighbours by warp
+ *                    shuffles: 28 outputs per warp (not for the mixed y sweep);
+ *   HB_KERNEL_COOP   a CTA of 4 warps takes 128 consecutive cells of a line,
+ *                    neighbours through shared memory: 124 outputs per CTA;
+ *   HB_KERNEL_COOP8  the same with 8 warps: 252 outputs per CTA;
+ *   HB_KERNEL_AUTO   the measured default for the grid size.
+ * get_kernel returns the current choice (-1 on error). */
+#define HB_KERNEL_AUTO (-1)
+#define HB_KERNEL_MARCH 0
+#define HB_KERNEL_WARP 1
+#define HB_KERNEL_COOP 2
+#define HB_KERNEL_COOP8 3
+int hydro_b200_domain_set_kernel(hb_domain *d, int precision, int idim, int kernel);
+int hydro_b200_domain_get_kernel(hb_domain *d, int precision, int idim);
 
 /* Event timing of every sweep launch: enable, then read the accumulated
  * milliseconds and launch counts of x (index 0) and y (index 1) sweeps. */

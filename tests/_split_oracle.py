@@ -40,6 +40,7 @@ class OracleSubdomain:
         self.p = orc_param_of(H)
         self.u = np.ascontiguousarray(u_local, dtype=np.float64).copy()
         self.send, self.recv = {}, {}
+        self.parts = []
         for idim in (1, 2):
             n = 8 * (H.ny if idim == 1 else H.nx)
             for side in (0, 1):
@@ -51,7 +52,16 @@ class OracleSubdomain:
         _, cx, cy = O.courant(self.p, self.u)
         return cx, cy
 
-    def sweep(self, stage, idim, dt, fuse):
+    def sweep(self, stage, idim, dt, fuse, part=0):
+        """part 0: the sweep.  The oracle sweeps whole lines, so the two parts
+        of an overlapped sweep are: part 1, which must run before the unpack,
+        records its place; part 2, after the unpack, sweeps."""
+        if part == 1:
+            self.parts.append((idim, "ghost-free"))
+            return
+        if part == 2:
+            assert self.parts and self.parts[-1] == (idim, "ghost-free")
+            self.parts.append((idim, "edges"))
         O.sweep(self.p, idim, dt, self.u)
 
     def pack(self, stage, idim, side):

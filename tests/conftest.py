@@ -7,6 +7,7 @@ import os
 import subprocess
 import sys
 
+import numpy as np
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -52,3 +53,23 @@ def oracle():
     from oracle import oracle as O
     O.oracle_lib()
     return O
+
+
+@pytest.fixture(scope="session")
+def reference_4096_200(oracle):
+    """The 4096^2 centred blast's whole 200-step run by the reference's own
+    C99/OpenMP code (oracle/_ref, compiled from the reference sources) on all
+    host cores, computed once per session: (state, dt sequence, final t).
+    Skips where the reference was not compiled."""
+    if not oracle.ref_available():
+        pytest.skip("oracle/_ref (the reference compiled from its sources) is not built: "
+                    "the full-run tests need the reference itself")
+    from hydro_b200 import make_params
+    from _helpers import orc_from_H
+    H = make_params(4096, 4096, testcase=0)
+    ref = oracle.RefState(orc_from_H(oracle, H), 0)
+    n, dts, t, _, _ = ref.run(200)
+    u = ref.get()
+    ref.close()
+    assert n == 200
+    return u, np.asarray(dts), t

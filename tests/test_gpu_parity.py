@@ -99,11 +99,16 @@ def test_device_loop_matches_oracle(product_lib, oracle, nx, ny, tc, nsteps, bnd
     (80, 50, 0, 30, (0, 1, 0, 1), {"iorder": 1, "scheme": 2}),
     (300, 64, 0, 30, (1, 1, 1, 1), {"slope_type": 0.5}),
 ])
-def test_marching_x_sweep_matches_oracle(product_lib, oracle, nx, ny, tc, nsteps, bnd, extra):
-    """The same, with the row-marching x-sweep kernel (shared-memory row ring)."""
+@pytest.mark.parametrize("kernels", [("march", "march"), ("coop", "coop"), ("coop8", "coop8"),
+                                     ("coop", "warp")])
+def test_kernel_variants_match_oracle(product_lib, oracle, nx, ny, tc, nsteps, bnd, extra,
+                                      kernels):
+    """The same with the other sweep kernels: row-marching x sweep (shared-
+    memory row ring) and marching y sweep, and the 4- and 8-warp cooperative
+    windows, on odd, ragged and 3-cell-thin grids."""
     H = make_params(nx, ny, boundary=bnd, testcase=tc, **extra)
     want, wdts, wt = run_oracle(oracle, H, tc, nsteps)
-    d = Domain(H, xsweep="march")
+    d = Domain(H, kernels=kernels)
     d.upload(init_state(H, tc))
     d.set_clock()
     d.launch_steps(nsteps)
@@ -240,14 +245,12 @@ def test_full_size_4096_first_steps_and_conservation(product_lib, oracle):
     assert np.all(np.isfinite(u)) and np.all(u[0, 2:-2, 2:-2] > 0)
 
 
-def test_full_size_4096_200_steps_against_the_reference(product_lib, oracle):
+def test_full_size_4096_200_steps_against_the_reference(product_lib, reference_4096_200):
     """The 4096^2 centred blast over its whole 200-step run, per cell and per
     dt, against the reference's own C99/OpenMP code (oracle/_ref, built from
     the reference sources), run on all host cores.  Skipped, not downgraded,
     where the reference was not compiled."""
-    if not oracle.ref_available():
-        pytest.skip("oracle/_ref (the reference compiled from its sources) is not built: "
-                    "the full-run parity test needs the reference itself")
+    want, wdts, wt = reference_4096_200
     H = make_params(4096, 4096, testcase=0)
     u0 = init_state(H)
     run = HydroRun(H, u0.copy())
@@ -255,12 +258,7 @@ def test_full_size_4096_200_steps_against_the_reference(product_lib, oracle):
     got = run.sync_to_host().copy()
     t_gpu = run.t
     run.close()
-    p = orc_from_H(oracle, H)
-    ref = oracle.RefState(p, 0)
-    n, wdts, wt, _, _ = ref.run(200)
-    want = ref.get()
-    ref.close()
-    assert n == 200 and len(dts) == 200
+    assert len(dts) == 200
     assert bitwise_equal(dts, wdts) and t_gpu == wt
     assert bitwise_equal(got, want), describe_mismatch(got, want)
 
@@ -274,18 +272,21 @@ def test_full_size_4096_200_steps_against_the_reference(product_lib, oracle):
     ("rough", 16, 96, 33, {"iorder": 1, "niter_riemann": 3}),
     ("vacuum", 17, 512, 384, {}),
 ])
-@pytest.mark.parametrize("xsweep", ["cell", "march"])
-def test_random_states_match_oracle(product_lib, oracle, kind, seed, nx, ny, extra, xsweep):
+@pytest.mark.parametrize("kernels", [("warp", "warp"), ("march", "march"), ("coop", "coop"),
+                                     ("coop8", "coop8")])
+def test_random_states_match_oracle(product_lib, oracle, kind, seed, nx, ny, extra, kernels):
     """Random states (shocks and rarefactions everywhere, near-vacuum cells,
-    negative internal energy; see _helpers.random_state) through both x-sweep
-    kernels: every cell and the final dt bit for bit against the oracle,
-    which is itself checked against the reference on such states."""
+    negative internal energy; see _helpers.random_state) through every sweep
+    kernel (marching segments, warp windows, 4- and 8-warp cooperative
+    windows, in both directions): every cell and the final dt bit for bit
+    against the oracle, which is itself checked against the reference on
+    such states."""
     from _helpers import random_state
     bnd = (1, 2, 3, 1) if seed % 2 else (1, 1, 1, 1)
     H = make_params(nx, ny, boundary=bnd, **extra)
     u0 = random_state(nx, ny, seed, kind)
     want, wdts, wt = run_oracle(oracle, H, 0, 16, u=u0)
-    d = Domain(H, xsweep=xsweep)
+    d = Domain(H, kernels=kernels)
     d.upload(u0)
     d.set_clock()
     d.launch_steps(16)

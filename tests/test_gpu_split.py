@@ -71,12 +71,17 @@ def test_halo_pack_unpack_layout(product_lib):
     (200, 120, 0, 3, (1, 2, 2, 1)),
     (1024, 1024, 0, 4, (1, 1, 1, 1)),
 ])
-def test_split_equals_single_grid_fp64(product_lib, gx, gy, tc, nparts, bnd):
+@pytest.mark.parametrize("overlap,kernels", [(False, None), (True, None),
+                                             (True, ("march", "march")), (True, ("coop", "coop"))])
+def test_split_equals_single_grid_fp64(product_lib, gx, gy, tc, nparts, bnd, overlap, kernels):
+    """With overlap, every sweep runs as its ghost-free windows before the
+    exchange and the other windows after the unpack, for each kind of sweep
+    kernel."""
     Hg = make_params(gx, gy, testcase=tc, boundary=bnd)
     u0 = init_state(Hg, tc)
     nsteps = 40
     want, dts, t = single(Hg, u0, nsteps, "fp64")
-    run = split_gpu_local(Hg, u0, nparts)
+    run = split_gpu_local(Hg, u0, nparts, overlap=overlap, kernels=kernels)
     assert run.run(nsteps) == nsteps
     got = gather_global(Hg, run.subs)
     m = outer_mask(Hg)
@@ -100,7 +105,8 @@ def test_split_equals_single_grid_mixed(product_lib):
         s.close()
 
 
-def test_nccl_driver_single_rank(product_lib, tmp_path):
+@pytest.mark.parametrize("overlap", [0, 1])
+def test_nccl_driver_single_rank(product_lib, tmp_path, overlap):
     """The torch.distributed driver on the GPU with NCCL, one rank: the dt
     all-reduce runs on the subdomain's stream and the run equals the
     single-grid run bit for bit.  (Halo exchanges between ranks need two GPUs;
@@ -122,7 +128,7 @@ u0 = init_state(Hg)
 box = decompose(Hg.nx, Hg.ny, 1)[0]
 sub = GpuSubdomain(local_params(Hg, box, 0, 1), box, 0, "cuda:0")
 sub.upload(scatter_state(u0, box))
-run = SplitRun(Hg, [sub], DistComm())
+run = SplitRun(Hg, [sub], DistComm(), overlap=bool(int(sys.argv[2])))
 run.run(24)
 got = sub.download()
 sub.close()
@@ -133,8 +139,8 @@ dist.destroy_process_group()
 """
     env = dict(os.environ, RANK="0", LOCAL_RANK="0", WORLD_SIZE="1", MASTER_ADDR="127.0.0.1",
                MASTER_PORT=str(free_port()), NCCL_NVLS_ENABLE="0")
-    r = subprocess.run([sys.executable, "-c", code, ROOT], env=env, capture_output=True, text=True,
-                       timeout=300)
+    r = subprocess.run([sys.executable, "-c", code, ROOT, str(overlap)], env=env,
+                       capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr[-3000:]
     rec = json.loads(r.stdout.strip().splitlines()[-1])
     assert rec == {"equal": True, "t_equal": True}, rec

@@ -195,3 +195,36 @@ def test_request_larger_than_the_budget_is_rejected_not_blocking():
     st = Server(be, clock=clk, sleep=clk.sleep).run(reqs, max_wall_s=1e3)
     assert st.rejected == 1 and [c[0] for c in st.completed] == [2]
     assert st.summary()["rejected"] == 1
+
+
+def test_overload_reports_censored_requests_and_side_buckets():
+    """Under overload the stream is cut off with requests still queued and
+    running.  Every arrived, admissible request is either completed or
+    censored (with its age at the cutoff as a lower bound on its time to
+    solution), the lower-bound percentiles are at least the completed ones'
+    order statistics allow, and the side buckets partition both sets."""
+    clk = FakeClock()
+    be = SimBackend(clk, budget_cells=3 * 128 * 128, cost=1e-7)
+    reqs = poisson_requests(400, 500.0, seed=3, side_lo=64, side_hi=2048)
+    st = Server(be, clock=clk, sleep=clk.sleep).run(reqs, max_wall_s=0.5)
+    s = st.summary()
+    assert s["censored"]["count"] > 0 and s["censored"]["queued"] > 0
+    assert s["completed"] + s["censored"]["count"] + s["rejected"] == s["arrived"]
+    assert s["censored"]["running"] == s["running_end"]
+    for rid, age, state, cells in st.censored:
+        r = next(q for q in reqs if q.rid == rid)
+        assert abs(age - (st.wall_s - r.arrival)) < 1e-9 and state in ("queued", "running")
+    assert s["p50_lower_bound_s"] >= min(c[1] for c in st.completed)
+    assert s["censored"]["age_max_s"] <= st.wall_s
+    buckets = s["by_side"]
+    assert sum(b["completed"] for b in buckets.values()) == s["completed"]
+    assert sum(b["censored"] for b in buckets.values()) == s["censored"]["count"]
+
+
+def test_light_load_has_nothing_censored():
+    clk = FakeClock()
+    be = SimBackend(clk, budget_cells=10**6)
+    reqs = poisson_requests(20, 5.0, seed=5, side_lo=32, side_hi=128)
+    s = Server(be, clock=clk, sleep=clk.sleep).run(reqs, max_wall_s=1e6).summary()
+    assert s["censored"]["count"] == 0 and s["p50_lower_bound_s"] == s["p50_s"]
+    assert s["by_side"]["side<=256"]["completed"] == 20

@@ -109,15 +109,20 @@ def outer_mask(Hg):
     (48, 36, 0, 9, (2, 2, 2, 2)),
     (50, 30, 0, 3, (1, 2, 2, 1)),
 ])
-def test_local_split_equals_single_grid(gx, gy, tc, nproc, bnd):
+@pytest.mark.parametrize("overlap", [False, True])
+def test_local_split_equals_single_grid(gx, gy, tc, nproc, bnd, overlap):
+    """With overlap, each sweep is issued as its ghost-free part before the
+    halo exchange and its edge part after the unpack."""
     Hg = make_params(gx, gy, testcase=tc, boundary=bnd)
     u0 = init_state(Hg, tc)
     want, dts, t = single_run(Hg, u0, 24)
     boxes = decompose(gx, gy, nproc)
     subs = [OracleSubdomain(local_params(Hg, b, r, nproc), b, r, scatter_state(u0, b))
             for r, b in enumerate(boxes)]
-    run = SplitRun(Hg, subs, LocalComm())
+    run = SplitRun(Hg, subs, LocalComm(), overlap=overlap)
     assert run.run(24) == 24
+    if overlap:
+        assert all(len(s.parts) == 2 * 2 * 24 for s in subs)
     got = np.zeros_like(want)
     for s in subs:
         gather_into(got, s.download(), s.box)
@@ -133,7 +138,7 @@ import numpy as np, torch, torch.distributed as dist
 from hydro_b200 import init_state, make_params
 from hydro_b200.split import DistComm, SplitRun, decompose, gather_into, local_params, scatter_state
 from _split_oracle import OracleSubdomain
-gx, gy, tc, nsteps = (int(a) for a in sys.argv[2:6])
+gx, gy, tc, nsteps, overlap = (int(a) for a in sys.argv[2:7])
 dist.init_process_group("gloo", init_method="env://")
 rank, world = dist.get_rank(), dist.get_world_size()
 Hg = make_params(gx, gy, testcase=tc)
@@ -141,24 +146,28 @@ u0 = init_state(Hg, tc)
 boxes = decompose(gx, gy, world)
 sub = OracleSubdomain(local_params(Hg, boxes[rank], rank, world), boxes[rank], rank,
                       scatter_state(u0, boxes[rank]))
-run = SplitRun(Hg, [sub], DistComm())
+run = SplitRun(Hg, [sub], DistComm(), overlap=bool(overlap))
 run.run(nsteps)
+assert not overlap or len(sub.parts) == 4 * nsteps
 parts = [None] * world
 dist.all_gather_object(parts, sub.download())
 if rank == 0:
     g = np.zeros_like(u0)
     for r, ul in enumerate(parts):
         gather_into(g, ul, boxes[r])
-    np.save(sys.argv[6], g)
+    np.save(sys.argv[7], g)
     print(json.dumps({"t": run.t, "dts": run.dts}))
 dist.destroy_process_group()
 """
 
 
-@pytest.mark.parametrize("world,gx,gy,tc", [(2, 41, 27, 0), (3, 50, 23, 2), (4, 36, 30, 1)])
-def test_gloo_ranks_split_equals_single_grid(tmp_path, world, gx, gy, tc):
+@pytest.mark.parametrize("world,gx,gy,tc,overlap", [(2, 41, 27, 0, 0), (3, 50, 23, 2, 0),
+                                                    (4, 36, 30, 1, 0), (2, 41, 27, 0, 1),
+                                                    (4, 36, 30, 1, 1)])
+def test_gloo_ranks_split_equals_single_grid(tmp_path, world, gx, gy, tc, overlap):
     out = str(tmp_path / "g.npy")
-    outs = run_ranks(WORKER, world=world, extra_args=(str(gx), str(gy), str(tc), "16", out))
+    outs = run_ranks(WORKER, world=world,
+                     extra_args=(str(gx), str(gy), str(tc), "16", str(overlap), out))
     rec = json.loads(outs[0].strip().splitlines()[-1])
     Hg = make_params(gx, gy, testcase=tc)
     want, dts, t = single_run(Hg, init_state(Hg, tc), 16)
