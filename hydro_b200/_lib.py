@@ -167,9 +167,9 @@ SIGNATURES = [
     ("hydro_b200_batch_global_step", C.c_longlong, [_D]),
     ("hydro_b200_batch_launch_count", C.c_longlong, [_D]),
     ("hydro_b200_batch_stream", C.c_void_p, [_D]),
-    ("hydro_b200_batch_set_tuning", C.c_int, [_D, C.c_int, C.c_int, C.c_int]),
+    ("hydro_b200_batch_set_tuning", C.c_int, [_D, C.c_int, C.c_int, C.c_int, C.c_int]),
     ("hydro_b200_batch_get_tuning", C.c_int, [_D, C.POINTER(C.c_int), C.POINTER(C.c_int),
-                                              C.POINTER(C.c_int)]),
+                                              C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     ("hydro_b200_batch_autotune", C.c_int, [_D, C.c_int]),
     ("hydro_b200_set_device", C.c_int, [C.c_int]),
     ("hydro_b200_godunov_noalloc", C.c_int, [_P, C.c_void_p, C.c_int, C.c_double, C.c_void_p]),

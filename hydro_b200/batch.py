@@ -163,13 +163,14 @@ class Batch:
     def launch_count(self) -> int:
         return int(self.lib.hydro_b200_batch_launch_count(self.h))
 
-    def set_tuning(self, seg: int, claim: int, blocks_per_sm: int = 0) -> None:
-        check(self.lib.hydro_b200_batch_set_tuning(self.h, seg, claim, blocks_per_sm))
+    def set_tuning(self, seg: int, claim: int, blocks_per_sm: int = 0, threads: int = 64) -> None:
+        check(self.lib.hydro_b200_batch_set_tuning(self.h, seg, claim, blocks_per_sm, threads))
 
     def tuning(self):
-        s, c, b = C.c_int(), C.c_int(), C.c_int()
-        check(self.lib.hydro_b200_batch_get_tuning(self.h, C.byref(s), C.byref(c), C.byref(b)))
-        return {"seg": s.value, "claim": c.value, "blocks_per_sm": b.value}
+        s, c, b, t = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        check(self.lib.hydro_b200_batch_get_tuning(self.h, C.byref(s), C.byref(c), C.byref(b),
+                                                   C.byref(t)))
+        return {"seg": s.value, "claim": c.value, "blocks_per_sm": b.value, "threads": t.value}
 
     def autotune(self, steps: int = 2) -> int:
         n = self.lib.hydro_b200_batch_autotune(self.h, steps)

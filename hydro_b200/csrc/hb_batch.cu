@@ -43,6 +43,7 @@ struct Tuning {
     int seg = 64;          // y-segment length of y items
     int claim = 4;         // items per claim
     int blocks_per_sm = 0; // persistent CTAs per SM (0: occupancy limit)
+    int threads = 64;      // threads per CTA (columns per y item)
 };
 
 std::mutex g_tune_mu;
@@ -173,7 +174,7 @@ int build_lists(hb_batch* b) {
         if (b->off[s] < 0 || !I.active) continue;
         const bool even = (I.nstep % 2) == 0;
         const int xl = even ? 0 : 1, yl = 1 - xl;
-        for (int l0 = 0; l0 < I.nx; l0 += hb::kBatchThreads)
+        for (int l0 = 0; l0 < I.nx; l0 += b->tune.threads)
             for (int k0 = 2; k0 < I.ny + 2; k0 += b->tune.seg)
                 L[yl][1].push_back(WorkItem{s, 2, l0, k0});
         // x windows of the stage set's width (two cells per lane in mixed precision)
@@ -202,7 +203,7 @@ int build_lists(hb_batch* b) {
 
 int grid_size(hb_batch* b, int dir) {
     const int occ = hb::batch_sweep_blocks_per_sm(b->precision == HB_PREC_MIXED,
-                                                  b->P.unit_slope != 0, dir);
+                                                  b->P.unit_slope != 0, dir, b->tune.threads);
     const int per = (b->tune.blocks_per_sm > 0 && b->tune.blocks_per_sm < occ)
                         ? b->tune.blocks_per_sm
                         : occ;
@@ -219,6 +220,7 @@ int launch_sweep(hb_batch* b, int list, int phase, cudaStream_t s) {
         L.counter = b->counters + 2 * (phase - 1) + (dir - 1);
         L.seg = b->tune.seg;
         L.claim = b->tune.claim;
+        L.threads = b->tune.threads;
         if (L.nitems == 0) continue;
         const int grid = grid_size(b, dir);
         HB_BCU(b->precision == HB_PREC_MIXED
@@ -601,28 +603,32 @@ extern "C" int hydro_b200_batch_download(hb_batch* b, int slot, double* host) {
 extern "C" long long hydro_b200_batch_global_step(hb_batch* b) { return b ? b->gstep : -1; }
 extern "C" long long hydro_b200_batch_launch_count(hb_batch* b) { return b ? b->launches : 0; }
 
-extern "C" int hydro_b200_batch_set_tuning(hb_batch* b, int seg, int claim, int blocks_per_sm) {
-    if (!b || seg < 8 || claim < 1 || blocks_per_sm < 0)
+extern "C" int hydro_b200_batch_set_tuning(hb_batch* b, int seg, int claim, int blocks_per_sm,
+                                           int threads) {
+    if (!b || seg < 8 || claim < 1 || blocks_per_sm < 0 || (threads != 64 && threads != 128))
         return fail(HB_ERR_ARG, "set_tuning: invalid values");
     b->tune.seg = seg;
     b->tune.claim = claim;
     b->tune.blocks_per_sm = blocks_per_sm;
+    b->tune.threads = threads;
     b->lists_dirty = true;
     b->graphs_dirty = true;
     return HB_OK;
 }
 
 extern "C" int hydro_b200_batch_get_tuning(hb_batch* b, int* seg, int* claim,
-                                           int* blocks_per_sm) {
+                                           int* blocks_per_sm, int* threads) {
     if (!b) return fail(HB_ERR_ARG, "get_tuning: null batch");
     if (seg) *seg = b->tune.seg;
     if (claim) *claim = b->tune.claim;
     if (blocks_per_sm) *blocks_per_sm = b->tune.blocks_per_sm;
+    if (threads) *threads = b->tune.threads;
     return HB_OK;
 }
 
-// Tile autotuner: times `steps` real global steps per candidate tiling (the
-// tiling does not change any result, so the steps are not wasted) and keeps
+// Tile autotuner: times `steps` real global steps per candidate tiling --
+// threads per CTA (64, 128), y-segment length, items per claim, CTAs per SM
+// -- (the tiling does not change any result, so the steps are not wasted) and keeps
 // the fastest; remembered per shape signature for later batches.  Returns the
 // number of global steps it advanced.
 extern "C" int hydro_b200_batch_autotune(hb_batch* b, int steps) {
@@ -640,33 +646,35 @@ extern "C" int hydro_b200_batch_autotune(hb_batch* b, int steps) {
     }
     static const int segs[] = {32, 64, 128};
     static const int claims[] = {1, 4, 16};
-    const int occ = hb::batch_sweep_blocks_per_sm(b->precision == HB_PREC_MIXED,
-                                                  b->P.unit_slope != 0, 2);
-    const int bpsms[] = {0, std::max(1, occ / 2)};
     cudaEvent_t e0, e1;
     if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
         return fail(HB_ERR_CUDA, "autotune events"), -1;
     Tuning best = b->tune;
     float best_ms = 1e30f;
     int advanced = 0;
-    for (int sg : segs)
-        for (int cl : claims)
-            for (int bp : bpsms) {
-                b->tune = Tuning{sg, cl, bp};
-                b->lists_dirty = b->graphs_dirty = true;
-                if (prepare(b) != HB_OK) return -1;
-                cudaEventRecord(e0, b->stream);
-                if (hydro_b200_batch_steps(b, steps) != HB_OK) return -1;
-                cudaEventRecord(e1, b->stream);
-                cudaEventSynchronize(e1);
-                float ms = 0.f;
-                cudaEventElapsedTime(&ms, e0, e1);
-                advanced += steps;
-                if (ms < best_ms) {
-                    best_ms = ms;
-                    best = b->tune;
+    for (int th : hb::kBatchThreadChoices) {
+        const int occ = hb::batch_sweep_blocks_per_sm(b->precision == HB_PREC_MIXED,
+                                                      b->P.unit_slope != 0, 2, th);
+        const int bpsms[] = {0, std::max(1, occ / 2)};
+        for (int sg : segs)
+            for (int cl : claims)
+                for (int bp : bpsms) {
+                    b->tune = Tuning{sg, cl, bp, th};
+                    b->lists_dirty = b->graphs_dirty = true;
+                    if (prepare(b) != HB_OK) return -1;
+                    cudaEventRecord(e0, b->stream);
+                    if (hydro_b200_batch_steps(b, steps) != HB_OK) return -1;
+                    cudaEventRecord(e1, b->stream);
+                    cudaEventSynchronize(e1);
+                    float ms = 0.f;
+                    cudaEventElapsedTime(&ms, e0, e1);
+                    advanced += steps;
+                    if (ms < best_ms) {
+                        best_ms = ms;
+                        best = b->tune;
+                    }
                 }
-            }
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     b->tune = best;

@@ -8,7 +8,7 @@
 // sweep launches that pull work items of all instances from a queue, and a
 // clock kernel (t += dt, nstep++).  Work items are CTA-sized: an x item is
 // one row's run of cell windows (cell-per-lane x sweep), a y item is a group
-// of 64 columns over one row segment (marching y sweep).  Instances need not
+// of columns (one per thread of a CTA) over one row segment (marching y sweep).  Instances need not
 // share the sweep order: each instance's first sweep is x on its even steps
 // and y on its odd ones, so the host builds two item lists from the
 // instances' step parities and the launches alternate them.
@@ -40,32 +40,33 @@ struct BatchInst {
 struct WorkItem {
     int slot;
     int dir;   // 1: x item (row, first window), 2: y item (first column, first row)
-    int line;  // x: interior row l; y: first interior column l of the 64-column group
+    int line;  // x: interior row l; y: first interior column l of the column group
     int k0;    // x: first cell window; y: first output cell (row) of the segment
 };
 
-constexpr int kBatchThreads = 64;   // CTA of the batched sweep (two warps)
+// Threads per CTA of the batched sweep (the autotuner's "threads per tile"):
+// 64 or 128.  A y item is a group of that many columns over one row segment;
+// an x item's windows are shared by the CTA's warps.
+constexpr int kBatchThreadChoices[2] = {64, 128};
 constexpr int kBatchCourSlots = 16; // Courant accumulator slots per instance
-// Resident CTAs per SM the x-item kernels are compiled for: a register cap
-// (72 registers) that keeps the cell-per-lane work near the occupancy of the
-// plain x sweep.  Measured on the 256-instance batch: 10 (96 registers) leaves
-// the kernel latency-bound; 14 is 5% faster per step in both precisions, 16
-// slower again.
-constexpr int kBatchXMinBlocks = 14;
-// The mixed-precision x-item kernel (two cells per lane) takes the plain mixed
-// x sweep's cap.  It must: the mixed code is built with FMA contraction, and
-// which multiply-adds get fused depends on the context the window is compiled
-// in, register budget included, so the same window under different caps
-// rounds differently.  With equal caps a batched instance is bitwise equal to
-// its single-grid run; the tests check it, since any change to the code
-// around the window can break it.
-constexpr int kBatchXMixedMinBlocks = kMixedCellMinBlocks;
-// The same for the mixed-precision y-item kernel (marching, prefetching):
-// uncapped it takes 147 registers (6 CTAs per SM); 7 CTAs is 3% faster per
-// batched step, 8 less so.
-constexpr int kBatchYMixedMinBlocks = 7;
-// The FP64 y-item kernel takes the plain FP64 march's cap (kFp64MarchMinBlocks,
-// 64 registers): 134 registers uncapped, 15% slower per batched step.
+// Resident threads per SM the item kernels are compiled for (register caps,
+// as minimum CTAs per SM = threads / CTA size), measured on the 256-instance
+// batch:
+//  - FP64 x items: 896 (72 registers); uncapped (96 registers) they are
+//    latency-bound, and 14 CTAs of 64 are 5% faster per step than 10.
+//  - FP64 y items: 1024, the plain FP64 march's cap (64 registers): 134
+//    registers uncapped, 15% slower per batched step.
+//  - mixed x items: 768 (80 registers), the plain mixed x sweep's.
+//  - mixed y items (marching, prefetching): 448; uncapped they take 147
+//    registers (6 CTAs of 64), 7 CTAs of 64 are 3% faster, 8 less so.
+// The caps need not match the single-grid kernels': no stage set rounds
+// differently in another kernel (the FP64 set rounds every operation once,
+// the mixed set writes its fused multiply-adds out), so batched instances
+// equal their single-grid runs bit for bit under any cap or CTA size.
+constexpr int kBatchXThreadsPerSm = 896;
+constexpr int kBatchYThreadsPerSm = 1024;
+constexpr int kBatchXMixedThreadsPerSm = 768;
+constexpr int kBatchYMixedThreadsPerSm = 448;
 constexpr int kXItemWindows = 8;    // cell windows per x item (4 per warp)
 
 struct BatchLaunch {
@@ -76,15 +77,17 @@ struct BatchLaunch {
     unsigned int* counter;     // claim counter, zero before the launch
     int seg;                   // y-segment length used to build the items
     int claim;                 // items claimed per atomic
+    int threads;               // threads per CTA (one of kBatchThreadChoices)
 };
 
 // Launchers (hb_kernels.cu for FP64, hb_mixed.cu for the mixed form).
-// One launch sweeps the items of one direction (dir 1: x, 2: y).
+// One launch sweeps the items of one direction (dir 1: x, 2: y) with
+// L.threads threads per CTA.
 cudaError_t launch_batch_sweep(const BatchLaunch& L, const Phys& P, int dir, int grid,
                                cudaStream_t s);
 cudaError_t launch_batch_sweep_mixed(const BatchLaunch& L, const Phys& P, int dir, int grid,
                                      cudaStream_t s);
-int batch_sweep_blocks_per_sm(bool mixed, bool unit_slope, int dir);
+int batch_sweep_blocks_per_sm(bool mixed, bool unit_slope, int dir, int threads);
 cudaError_t launch_batch_clock_begin(BatchInst* inst, int nslots, double courant_factor,
                                      double smallc, long long* gstep, cudaStream_t s);
 cudaError_t launch_batch_clock_end(BatchInst* inst, int nslots, long long* gstep,

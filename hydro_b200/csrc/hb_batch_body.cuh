@@ -41,11 +41,11 @@ __device__ __forceinline__ SweepArgs batch_args(const BatchInst& I, int dir, int
 
 // Persistent CTAs claim `claim` items at a time until the list is exhausted;
 // every item of the list sweeps direction DIR (x: cell-per-lane windows of a
-// row, y: marching 64-column groups), so each direction has its own kernel
+// row, y: marching groups of T columns), so each direction has its own kernel
 // with its own register budget.  An item's instance is skipped once its clock
 // has stopped.  The second sweep of an instance's odd step also reduces its
 // Courant maxima.
-template <class S, int DIR>
+template <class S, int DIR, int T>
 __device__ __forceinline__ void batch_sweep_body(const BatchLaunch& L, const Phys& P) {
     __shared__ int s_base;
     const typename S::Consts C = S::consts(P);
@@ -67,7 +67,7 @@ __device__ __forceinline__ void batch_sweep_body(const BatchLaunch& L, const Phy
             double cx = 0.0, cy = 0.0;
             if (DIR == 1) {
                 const int warp = threadIdx.x >> 5;
-                for (int win = w.k0 + warp; win < w.k0 + kXItemWindows; win += kBatchThreads / 32)
+                for (int win = w.k0 + warp; win < w.k0 + kXItemWindows; win += T / 32)
                     xcell_window<S>(a, C, w.line, win, dtdx, cx, cy);
             } else {
                 const int l = w.line + threadIdx.x;

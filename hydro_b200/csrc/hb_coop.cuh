@@ -58,7 +58,6 @@ __device__ __forceinline__ void coop_window(const SweepArgs& a, const typename S
                                             double& cx, double& cy, CoopSmem<S, G>& sm) {
     using Prim = typename S::Prim;
     using Flux = typename S::Flux;
-    using Real = typename S::Real;
     constexpr int T = 32 * G, N = T - 4;
     const int t = threadIdx.x;
     const int c = win * N;                          // first output cell of the window
@@ -72,7 +71,7 @@ __device__ __forceinline__ void coop_window(const SweepArgs& a, const typename S
 
     Cons u{1.0, 0.0, 0.0, 1.0};
     Prim q = S::zero_prim();
-    Real cs = Real(0);
+    typename S::Sound cs = S::zero_sound();
     if (work) {
         if (k >= 0 && k < a.n) u = load_cell<DIR>(a, g, k);
         S::prim(C, u, q, cs);

@@ -319,36 +319,47 @@ cudaError_t launch_clock_end(DevClock* c, cudaStream_t s) {
 }
 
 // ---------------------------------------------------------------- batches
-template <bool UNIT, int DIR>
-__global__ void __launch_bounds__(kBatchThreads, DIR == 1 ? kBatchXMinBlocks : kFp64MarchMinBlocks)
+template <bool UNIT, int DIR, int T>
+__global__ void __launch_bounds__(T, (DIR == 1 ? kBatchXThreadsPerSm : kBatchYThreadsPerSm) / T)
 batch_sweep_kernel(const BatchLaunch L, const Phys P) {
-    batch_sweep_body<ExactStages<UNIT>, DIR>(L, P);
+    batch_sweep_body<ExactStages<UNIT>, DIR, T>(L, P);
+}
+
+template <bool UNIT, int T>
+static void launch_batch_t(const BatchLaunch& L, const Phys& P, int dir, int grid,
+                           cudaStream_t s) {
+    if (dir == 1) batch_sweep_kernel<UNIT, 1, T><<<grid, T, 0, s>>>(L, P);
+    else batch_sweep_kernel<UNIT, 2, T><<<grid, T, 0, s>>>(L, P);
 }
 
 cudaError_t launch_batch_sweep(const BatchLaunch& L, const Phys& P, int dir, int grid,
                                cudaStream_t s) {
-    if (dir == 1) {
-        if (P.unit_slope) batch_sweep_kernel<true, 1><<<grid, kBatchThreads, 0, s>>>(L, P);
-        else batch_sweep_kernel<false, 1><<<grid, kBatchThreads, 0, s>>>(L, P);
+    if (L.threads == 128) {
+        if (P.unit_slope) launch_batch_t<true, 128>(L, P, dir, grid, s);
+        else launch_batch_t<false, 128>(L, P, dir, grid, s);
     } else {
-        if (P.unit_slope) batch_sweep_kernel<true, 2><<<grid, kBatchThreads, 0, s>>>(L, P);
-        else batch_sweep_kernel<false, 2><<<grid, kBatchThreads, 0, s>>>(L, P);
+        if (P.unit_slope) launch_batch_t<true, 64>(L, P, dir, grid, s);
+        else launch_batch_t<false, 64>(L, P, dir, grid, s);
     }
     return cudaGetLastError();
 }
 
 template <class K>
-static int occupancy(K kernel) {
+static int occupancy(K kernel, int threads) {
     int n = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, kBatchThreads, 0);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, 0);
     return (e == cudaSuccess && n > 0) ? n : 1;
 }
 
-int batch_sweep_blocks_per_sm_exact(bool unit_slope, int dir) {
-    if (dir == 1) return unit_slope ? occupancy(batch_sweep_kernel<true, 1>)
-                                    : occupancy(batch_sweep_kernel<false, 1>);
-    return unit_slope ? occupancy(batch_sweep_kernel<true, 2>)
-                      : occupancy(batch_sweep_kernel<false, 2>);
+template <bool UNIT, int T>
+static int batch_occ(int dir) {
+    return dir == 1 ? occupancy(batch_sweep_kernel<UNIT, 1, T>, T)
+                    : occupancy(batch_sweep_kernel<UNIT, 2, T>, T);
+}
+
+int batch_sweep_blocks_per_sm_exact(bool unit_slope, int dir, int threads) {
+    if (threads == 128) return unit_slope ? batch_occ<true, 128>(dir) : batch_occ<false, 128>(dir);
+    return unit_slope ? batch_occ<true, 64>(dir) : batch_occ<false, 64>(dir);
 }
 
 // main.c:349-392 per instance (see clock_begin_kernel).

@@ -153,14 +153,15 @@ struct RowRing {
 };
 
 // The march of one thread over [k0, k1); S::Prim / S::Flux are the stage set's
-// primitive and flux records, S::Real its sound-speed type.
+// primitive and flux records, S::Sound what its primitives step hands to its
+// trace step (the sound speed, with reciprocals in the mixed set).
 template <int DIR, class S>
 __device__ __forceinline__ void march(const SweepArgs& a, const typename S::Consts& C,
                                       const LineGeom<DIR>& g, int k0, int k1, double dtdx,
                                       double& cx, double& cy) {
     using Prim = typename S::Prim;
     using Flux = typename S::Flux;
-    using Real = typename S::Real;
+    using Sound = typename S::Sound;
     const typename S::TraceK K = S::trace_constants(C, dtdx);
 
     __shared__ double ring_mem[DIR == 1 ? 4 : 1][8][kSweepThreads];
@@ -173,7 +174,7 @@ __device__ __forceinline__ void march(const SweepArgs& a, const typename S::Cons
                         ((a.vs & 1) == 0) && ((g.base & 1) == 0) && (((k0 - 2) & 1) == 0);
 
     Prim q1 = S::zero_prim(), q2 = S::zero_prim();  // primitives of k-1, k-2
-    Real c1 = Real(0);                              // sound speed of k-1
+    Sound c1 = S::zero_sound();                     // sound speed of k-1
     Prim xm2 = S::zero_prim();                      // qxm of k-2
     Flux fprev = S::zero_flux();                    // flux at (k-3 | k-2)
 
@@ -200,7 +201,7 @@ __device__ __forceinline__ void march(const SweepArgs& a, const typename S::Cons
             uk = load_cell<DIR>(a, g, k);
         }
         Prim qk;
-        Real ck;
+        Sound ck;
         S::prim(C, uk, qk, ck);
         Prim xm1 = xm2;
         Flux f = fprev;
@@ -307,7 +308,7 @@ __device__ __forceinline__ void line_window_1(const SweepArgs& a, const typename
                                              double& cy) {
     using Prim = typename S::Prim;
     using Flux = typename S::Flux;
-    using Real = typename S::Real;
+    using Sound = typename S::Sound;
     const int lane = threadIdx.x & 31;
     const int c = win * kCellWarpOut;                // first output cell of the warp
     if (c >= a.n - 2) return;                        // warp-uniform
@@ -317,7 +318,7 @@ __device__ __forceinline__ void line_window_1(const SweepArgs& a, const typename
     const bool inside = k >= 0 && k < a.n;           // lanes outside the row idle
     const Cons u = inside ? load_cell<DIR>(a, g, k) : Cons{1.0, 0.0, 0.0, 1.0};
     Prim q;
-    Real cs;
+    Sound cs;
     S::prim(C, u, q, cs);
     const Prim qm = prim_up(q), qp = prim_down(q);
     Prim dq = S::zero_prim();
@@ -363,7 +364,7 @@ __device__ __forceinline__ void xcell_window_2(const SweepArgs& a, const typenam
                                                double& cy) {
     using Prim = typename S::Prim;
     using Flux = typename S::Flux;
-    using Real = typename S::Real;
+    using Sound = typename S::Sound;
     const int lane = threadIdx.x & 31;
     const int c = win * kCellWarpOut2;               // first output cell of the warp
     if (c >= a.n - 2) return;                        // warp-uniform
@@ -373,7 +374,7 @@ __device__ __forceinline__ void xcell_window_2(const SweepArgs& a, const typenam
     const Cons ua = (ka >= 0 && ka < a.n) ? load_cell<1>(a, g, ka) : Cons{1.0, 0.0, 0.0, 1.0};
     const Cons ub = (kb >= 0 && kb < a.n) ? load_cell<1>(a, g, kb) : Cons{1.0, 0.0, 0.0, 1.0};
     Prim qa, qb;
-    Real ca, cb;
+    Sound ca, cb;
     S::prim(C, ua, qa, ca);
     S::prim(C, ub, qb, cb);
     const Prim qm = prim_up(qb), qp = prim_down(qa);  // cells ka - 1, kb + 1

@@ -1,6 +1,7 @@
 // hb_mixed.cu -- the mixed-precision sweep kernel (stage set in
 // hb_stages_mixed.cuh, march skeleton in hb_march.cuh).  Built with fast FP32
-// division / square root and FMA contraction (see the Makefile).
+// division / square root and no FMA contraction: the stage code writes its
+// fused multiply-adds out (see the Makefile).
 #include "hb_kernels.cuh"
 #include "hb_march.cuh"
 #include "hb_coop.cuh"
@@ -76,16 +77,22 @@ int sweep_mixed_blocks_per_sm(int dir) {
     return (e == cudaSuccess && n > 0) ? n : 1;
 }
 
-template <int DIR>
-__global__ void __launch_bounds__(kBatchThreads, DIR == 1 ? kBatchXMixedMinBlocks : kBatchYMixedMinBlocks)
+template <int DIR, int T>
+__global__ void __launch_bounds__(T, (DIR == 1 ? kBatchXMixedThreadsPerSm
+                                               : kBatchYMixedThreadsPerSm) / T)
 batch_sweep_mixed_kernel(const BatchLaunch L, const Phys P) {
-    batch_sweep_body<MixedStages, DIR>(L, P);
+    batch_sweep_body<MixedStages, DIR, T>(L, P);
 }
 
 cudaError_t launch_batch_sweep_mixed(const BatchLaunch& L, const Phys& P, int dir, int grid,
                                      cudaStream_t s) {
-    if (dir == 1) batch_sweep_mixed_kernel<1><<<grid, kBatchThreads, 0, s>>>(L, P);
-    else batch_sweep_mixed_kernel<2><<<grid, kBatchThreads, 0, s>>>(L, P);
+    if (L.threads == 128) {
+        if (dir == 1) batch_sweep_mixed_kernel<1, 128><<<grid, 128, 0, s>>>(L, P);
+        else batch_sweep_mixed_kernel<2, 128><<<grid, 128, 0, s>>>(L, P);
+    } else {
+        if (dir == 1) batch_sweep_mixed_kernel<1, 64><<<grid, 64, 0, s>>>(L, P);
+        else batch_sweep_mixed_kernel<2, 64><<<grid, 64, 0, s>>>(L, P);
+    }
     return cudaGetLastError();
 }
 
@@ -118,16 +125,21 @@ cudaError_t launch_batch_courant_mixed(BatchInst* inst, const int* slots, int ns
     return cudaGetLastError();
 }
 
-int batch_sweep_blocks_per_sm_exact(bool unit_slope, int dir);  // hb_kernels.cu
+int batch_sweep_blocks_per_sm_exact(bool unit_slope, int dir, int threads);  // hb_kernels.cu
 
-int batch_sweep_blocks_per_sm(bool mixed, bool unit_slope, int dir) {
-    if (!mixed) return batch_sweep_blocks_per_sm_exact(unit_slope, dir);
+template <int T>
+static int batch_mixed_occ(int dir) {
     int n = 0;
     cudaError_t e = dir == 1 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                                   &n, batch_sweep_mixed_kernel<1>, kBatchThreads, 0)
+                                   &n, batch_sweep_mixed_kernel<1, T>, T, 0)
                              : cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                                   &n, batch_sweep_mixed_kernel<2>, kBatchThreads, 0);
+                                   &n, batch_sweep_mixed_kernel<2, T>, T, 0);
     return (e == cudaSuccess && n > 0) ? n : 1;
+}
+
+int batch_sweep_blocks_per_sm(bool mixed, bool unit_slope, int dir, int threads) {
+    if (!mixed) return batch_sweep_blocks_per_sm_exact(unit_slope, dir, threads);
+    return threads == 128 ? batch_mixed_occ<128>(dir) : batch_mixed_occ<64>(dir);
 }
 
 }  // namespace hb

@@ -65,6 +65,22 @@ __device__ __forceinline__ double zdiv(double a, double b) {
     return a / b;
 }
 
+// sqrt(x) for an x that often equals x0 > 0 whose square root r0 is already
+// known (a Riemann problem between equal states evaluates W = sqrt(c (1 + 0))
+// four times with the c of its first guess): x == x0 means the same bits, so
+// r0 is sqrt(x) exactly.
+__device__ __forceinline__ double sqrt_eq(double x, double x0, double r0) {
+    if (x == x0) return r0;
+    return sqrt(x);
+}
+
+// a / b for a b that is often exactly 1 (rho* = rho_o / (1 + 0) between equal
+// states): a / 1 is a.
+__device__ __forceinline__ double div1(double a, double b) {
+    if (b == 1.0) return a;
+    return a / b;
+}
+
 // constoprim.c:37-52 then equation_of_state.c:41-48.
 __device__ __forceinline__ void cons_to_prim(const Phys& P, const Cons& u, Prim& q, double& c) {
     double r = omax(u.d, P.smallr);
@@ -197,12 +213,13 @@ __device__ __forceinline__ Cons riemann_flux(const Phys& P, const Prim& ql, cons
     double cr = gamma * pr * rr;
     double wl = sqrt(cl);
     double wr = sqrt(cr);
+    const double wl0 = wl, wr0 = wr;  // sqrt(cl), sqrt(cr)
     double pstar = cfmax(((wr * pl + wl * pr) + wl * wr * (ul - ur)) / (wl + wr), 0.0);
 
     for (int iter = 0; iter < P.niter; iter++) {
         double pst = pstar;
-        double wwl = sqrt(cl * (1.0 + zdiv(gamma6 * (pst - pl), pl)));
-        double wwr = sqrt(cr * (1.0 + zdiv(gamma6 * (pst - pr), pr)));
+        double wwl = sqrt_eq(cl * (1.0 + zdiv(gamma6 * (pst - pl), pl)), cl, wl0);
+        double wwr = sqrt_eq(cr * (1.0 + zdiv(gamma6 * (pst - pr), pr)), cr, wr0);
         double swwl = wwl * wwl;
         double qlw = 2.0 * wwl * swwl / (swwl + cl);
         double qrw = 2.0 * wwr * (wwr * wwr) / ((wwr * wwr) + cr);
@@ -217,8 +234,8 @@ __device__ __forceinline__ Cons riemann_flux(const Phys& P, const Prim& ql, cons
         if (!(conv > 1e-6)) break;
     }
 
-    wr = sqrt(cr * (1.0 + zdiv(gamma6 * (pstar - pr), pr)));
-    wl = sqrt(cl * (1.0 + zdiv(gamma6 * (pstar - pl), pl)));
+    wr = sqrt_eq(cr * (1.0 + zdiv(gamma6 * (pstar - pr), pr)), cr, wr0);
+    wl = sqrt_eq(cl * (1.0 + zdiv(gamma6 * (pstar - pl), pl)), cl, wl0);
     double ustar = 0.5 * (ul + zdiv(pl - pstar, wl) + ur - zdiv(pr - pstar, wr));
     bool left = ustar > 0.0;
     double sgnm = left ? 1.0 : -1.0;
@@ -226,11 +243,15 @@ __device__ __forceinline__ Cons riemann_flux(const Phys& P, const Prim& ql, cons
     double uo = left ? ul : ur;
     double po = left ? pl : pr;
     double wo = left ? wl : wr;
-    double co = sqrt(fabs(gamma * po / ro));
-    co = cfmax(smallc, co);
-    double rstar = ro / (1.0 + zdiv(ro * (po - pstar), wo * wo));
+    const double co_raw = sqrt(fabs(gamma * po / ro));
+    double co = cfmax(smallc, co_raw);
+    double rstar = div1(ro, 1.0 + zdiv(ro * (po - pstar), wo * wo));
     rstar = cfmax(rstar, smallr);
-    double cstar = sqrt(fabs(gamma * pstar / rstar));
+    // With p* = p_o and rho* = rho_o (both positive: equal bits), c* repeats
+    // c_o's arithmetic on the same operands.
+    double cstar;
+    if (pstar == po && rstar == ro) cstar = co_raw;
+    else cstar = sqrt(fabs(gamma * pstar / rstar));
     cstar = cfmax(smallc, cstar);
     double spout = co - sgnm * uo;
     double spin = cstar - sgnm * ustar;
@@ -297,13 +318,15 @@ struct ExactStages {
     using Consts = Phys;
     using Prim = hb::Prim;
     using Flux = Cons;
-    using Real = double;
+    using Real = double;   // element type of Prim
+    using Sound = double;  // the sound speed, from prim to trace
     using TraceK = hb::TraceK;
     static constexpr bool prefetch = false;
     static constexpr int cells_per_lane = 1;  // x sweep window (hb_march.cuh)
     static __device__ __forceinline__ Consts consts(const Phys& P) { return P; }
     static __device__ __forceinline__ Prim zero_prim() { return Prim{0.0, 0.0, 0.0, 0.0}; }
     static __device__ __forceinline__ Flux zero_flux() { return Flux{0.0, 0.0, 0.0, 0.0}; }
+    static __device__ __forceinline__ Sound zero_sound() { return 0.0; }
     static __device__ __forceinline__ TraceK trace_constants(const Phys& P, double dtdx) {
         return hb::trace_constants(P.scheme, dtdx);
     }

@@ -41,7 +41,8 @@ struct FastStages {
     using Consts = FastConsts;
     using Prim = hb::Prim;
     using Flux = Cons;
-    using Real = double;
+    using Real = double;   // element type of Prim
+    using Sound = double;  // the sound speed, from prim to trace
     using TraceK = hb::TraceK;
     static constexpr bool prefetch = false;
     static constexpr int cells_per_lane = 1;
@@ -54,6 +55,7 @@ struct FastStages {
     }
     static __device__ __forceinline__ Prim zero_prim() { return Prim{0.0, 0.0, 0.0, 0.0}; }
     static __device__ __forceinline__ Flux zero_flux() { return Flux{0.0, 0.0, 0.0, 0.0}; }
+    static __device__ __forceinline__ Sound zero_sound() { return 0.0; }
     static __device__ __forceinline__ TraceK trace_constants(const Consts& C, double dtdx) {
         return hb::trace_constants(C.P.scheme, dtdx);
     }

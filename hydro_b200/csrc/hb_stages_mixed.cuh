@@ -8,9 +8,16 @@
 //         conservative update u + dt/dx (F_l - F_r) with the flux difference
 //         taken in FP64 from the FP32 fluxes, and the Courant speeds that feed
 //         the dt reduction.
-// The state in HBM stays FP64.  This translation unit is built with fast FP32
-// division / square root and FMA contraction; it is not bitwise comparable to
-// the reference and is validated by its L1 / Linf error against the FP64 path.
+// The state in HBM stays FP64.  It is not bitwise comparable to the reference
+// and is validated by its L1 / Linf error against the FP64 path.
+//
+// Every multiply-add that should fuse is written as fmaf / fma, and the
+// translation unit is built without FMA contraction (--fmad=false, with fast
+// FP32 division and square root): the compiler then fuses nothing on its own,
+// so each stage rounds the same way in every kernel that calls it, whatever
+// its register budget, thread count or surroundings.  A batched instance is
+// therefore bitwise equal to its single-grid run under any kernel, tiling or
+// launch shape.
 #pragma once
 
 #include "hb_kernels.cuh"
@@ -28,9 +35,18 @@ struct FluxF {
 
 struct MixedConsts {
     float gamma, gm1, smallr, smallc, smallp, gamma6, entho, slope_type;
+    float inv_slope;                          // 1 / slope_type (slope.c:44 divides)
+    int unit_slope;                           // slope_type == 1
     double gamma6d, smallppd;                 // Newton iteration
     double gammad, gm1d, smallrd, smallpd;    // Courant speeds
     int niter, iorder, scheme;
+};
+
+// What the primitives step hands to the trace step: the sound speed c with
+// 1/c and 1/rho, which the trace needs and prim has on hand (one reciprocal
+// square root gives c and 1/c).
+struct SoundF {
+    float c, ic, ir;
 };
 
 struct TraceKF {
@@ -41,7 +57,8 @@ struct MixedStages {
     using Consts = MixedConsts;
     using Prim = PrimF;
     using Flux = Cons;   // the FP32 flux converted once to FP64 (exact)
-    using Real = float;
+    using Real = float;     // element type of Prim
+    using Sound = SoundF;
     using TraceK = TraceKF;
     static constexpr bool prefetch = true;
     static constexpr int cells_per_lane = 2;  // x sweep window (hb_march.cuh)
@@ -56,6 +73,8 @@ struct MixedStages {
         C.gamma6 = (float)P.gamma6;
         C.entho = (float)P.entho;
         C.slope_type = (float)P.slope_type;
+        C.inv_slope = (float)(1.0 / P.slope_type);
+        C.unit_slope = P.unit_slope;
         C.gamma6d = P.gamma6;
         C.smallppd = P.smallpp;
         C.gammad = P.gamma;
@@ -69,6 +88,7 @@ struct MixedStages {
     }
     static __device__ __forceinline__ Prim zero_prim() { return Prim{0.f, 0.f, 0.f, 0.f}; }
     static __device__ __forceinline__ Flux zero_flux() { return Flux{0.0, 0.0, 0.0, 0.0}; }
+    static __device__ __forceinline__ Sound zero_sound() { return Sound{0.f, 0.f, 0.f}; }
     static __device__ __forceinline__ bool second_order(const Consts& C) { return C.iorder != 1; }
 
     static __device__ __forceinline__ TraceK trace_constants(const Consts& C, double dtdx) {
@@ -86,66 +106,74 @@ struct MixedStages {
         return k;
     }
 
-    static __device__ __forceinline__ void prim(const Consts& C, const Cons& u, Prim& q, float& c) {
+    static __device__ __forceinline__ void prim(const Consts& C, const Cons& u, Prim& q, Sound& c) {
         const float r = fmaxf((float)u.d, C.smallr);
         const float ir = 1.0f / r;
         const float un = (float)u.mn * ir;
         const float ut = (float)u.mt * ir;
-        const float eken = 0.5f * (un * un + ut * ut);
-        const float e = (float)u.e * ir - eken;
+        const float eken = 0.5f * fmaf(un, un, ut * ut);
+        const float e = fmaf((float)u.e, ir, -eken);
         const float p = fmaxf(C.gm1 * r * e, r * C.smallp);
         q = Prim{r, un, ut, p};
-        c = sqrtf(C.gamma * p * ir);
+        const float c2 = C.gamma * p * ir;
+        const float ic = rsqrtf(c2);
+        c = Sound{c2 * ic, ic, ir};
     }
 
-    static __device__ __forceinline__ float slope1(float st, float qm, float q0, float qp) {
-        const float dlft = st * (q0 - qm);
-        const float drgt = st * (qp - q0);
-        const float dcen = 0.5f * (dlft + drgt) / st;
+    // slope.c:37-50; with slope_type 1 the two scalings are skipped.
+    static __device__ __forceinline__ float slope1(const Consts& C, float qm, float q0, float qp) {
+        float dlft = q0 - qm, drgt = qp - q0, dcen;
+        if (C.unit_slope) {
+            dcen = 0.5f * (dlft + drgt);
+        } else {
+            dlft *= C.slope_type;
+            drgt *= C.slope_type;
+            dcen = 0.5f * (dlft + drgt) * C.inv_slope;
+        }
         const float lim = (dlft * drgt <= 0.f) ? 0.f : fminf(fabsf(dlft), fabsf(drgt));
         const float m = fminf(lim, fabsf(dcen));
         return dcen > 0.f ? m : -m;
     }
     static __device__ __forceinline__ void slope4(const Consts& C, const Prim& a, const Prim& b,
                                                   const Prim& c, Prim& dq) {
-        dq.r = slope1(C.slope_type, a.r, b.r, c.r);
-        dq.u = slope1(C.slope_type, a.u, b.u, c.u);
-        dq.v = slope1(C.slope_type, a.v, b.v, c.v);
-        dq.p = slope1(C.slope_type, a.p, b.p, c.p);
+        dq.r = slope1(C, a.r, b.r, c.r);
+        dq.u = slope1(C, a.u, b.u, c.u);
+        dq.v = slope1(C, a.v, b.v, c.v);
+        dq.p = slope1(C, a.p, b.p, c.p);
     }
 
+    // trace.c:63-123, with the factor -1/2 of the characteristic amplitudes
+    // folded into them once for both sides.
     static __device__ __forceinline__ void trace(const TraceK& K, const Prim& q, const Prim& dq,
-                                                 float cc, Prim& qxm, Prim& qxp) {
+                                                 const Sound& s, Prim& qxm, Prim& qxp) {
+        const float cc = s.c, icc = s.ic, ir = s.ir;
         const float csq = cc * cc;
-        const float ir = 1.0f / q.r;
-        const float icc = 1.0f / cc;
         const float rOcc = q.r * icc;
         const float OrOcc = cc * ir;
         const float dprcc = dq.p * ir * icc;
-        const float alpham = 0.5f * (dprcc - dq.u) * rOcc;
-        const float alphap = 0.5f * (dprcc + dq.u) * rOcc;
-        const float alpha0r = dq.r - dq.p * icc * icc;
-        const float alpha0v = dq.v;
+        const float hm = -0.25f * rOcc;                       // -1/2 * 1/2 rho/c
+        const float am0 = (dprcc - dq.u) * hm;                 // -alpham / 2
+        const float ap0 = (dprcc + dq.u) * hm;                 // -alphap / 2
+        const float azr0 = -0.5f * fmaf(-dq.p, icc * icc, dq.r);  // -alpha0r / 2
+        const float azv0 = -0.5f * dq.v;                       // -alpha0v / 2
         const float upcc = q.u + cc, umcc = q.u - cc;
-        const float upccx = upcc * K.dtdx, umccx = umcc * K.dtdx, ux = q.u * K.dtdx;
 
-        float spm = (umcc >= K.zeror) ? K.project : umccx + 1.f;
-        float spp = (upcc >= K.zeror) ? K.project : upccx + 1.f;
-        float spz = (q.u >= K.zeror) ? K.project : ux + 1.f;
-        float ap = -0.5f * spp * alphap, am = -0.5f * spm * alpham;
-        float azr = -0.5f * spz * alpha0r, azv = -0.5f * spz * alpha0v;
-        qxp = Prim{q.r + (ap + am + azr), q.u + (ap - am) * OrOcc, q.v + azv,
-                   q.p + (ap + am) * csq};
+        float spm = (umcc >= K.zeror) ? K.project : fmaf(umcc, K.dtdx, 1.f);
+        float spp = (upcc >= K.zeror) ? K.project : fmaf(upcc, K.dtdx, 1.f);
+        float spz = (q.u >= K.zeror) ? K.project : fmaf(q.u, K.dtdx, 1.f);
+        float ap = spp * ap0, am = spm * am0, azr = spz * azr0, azv = spz * azv0;
+        qxp = Prim{q.r + (ap + am + azr), fmaf(ap - am, OrOcc, q.u), q.v + azv,
+                   fmaf(ap + am, csq, q.p)};
 
-        spm = (umcc <= K.zerol) ? -K.project : umccx - 1.f;
-        spp = (upcc <= K.zerol) ? -K.project : upccx - 1.f;
-        spz = (q.u <= K.zerol) ? -K.project : ux - 1.f;
-        ap = -0.5f * spp * alphap;
-        am = -0.5f * spm * alpham;
-        azr = -0.5f * spz * alpha0r;
-        azv = -0.5f * spz * alpha0v;
-        qxm = Prim{q.r + (ap + am + azr), q.u + (ap - am) * OrOcc, q.v + azv,
-                   q.p + (ap + am) * csq};
+        spm = (umcc <= K.zerol) ? -K.project : fmaf(umcc, K.dtdx, -1.f);
+        spp = (upcc <= K.zerol) ? -K.project : fmaf(upcc, K.dtdx, -1.f);
+        spz = (q.u <= K.zerol) ? -K.project : fmaf(q.u, K.dtdx, -1.f);
+        ap = spp * ap0;
+        am = spm * am0;
+        azr = spz * azr0;
+        azv = spz * azv0;
+        qxm = Prim{q.r + (ap + am + azr), fmaf(ap - am, OrOcc, q.u), q.v + azv,
+                   fmaf(ap + am, csq, q.p)};
     }
 
     static __device__ __forceinline__ Flux riemann(const Consts& C, const Prim& ql, const Prim& qr) {
@@ -171,7 +199,8 @@ struct MixedStages {
             cr = C.gamma * pr * rr;
         }
         const float wl0 = sqrtf(cl), wr0 = sqrtf(cr);
-        const float p0 = fmaxf(((wr0 * pl + wl0 * pr) + wl0 * wr0 * (ul - ur)) / (wl0 + wr0), 0.f);
+        const float p0 =
+            fmaxf(fmaf(wl0 * wr0, ul - ur, fmaf(wr0, pl, wl0 * pr)) / (wl0 + wr0), 0.f);
 
         // Newton iteration on p* (FP64): W^2 = c (1 + gamma6 (p - p_K) / p_K),
         // u*_l = u_l - (p - p_l) / W_l, u*_r = u_r + (p - p_r) / W_r, step
@@ -187,7 +216,7 @@ struct MixedStages {
             const double usl = fma(-(pst - pld), il, uld);
             const double usr = fma(pst - prd, ir, urd);
             const double iql = 0.5 * (wl2 + cld) * (il * il * il);
-            const double iqr = 0.5 * (wr2 + crd) * (ir * ir * ir);
+            const double iqr = 0.5 * (wr2 + crd) * (ir * ir * ir);  // 1 / q = (W^2 + c) / (2 W^3)
             double delp = (usl - usr) * rcp64(iql + iqr);
             delp = delp > -pst ? delp : -pst;
             pst += delp;
@@ -195,32 +224,40 @@ struct MixedStages {
         }
         const float ps = (float)pst;
 
-        // Sampling (FP32).
-        const float wr = sqrtf(cr * (1.f + C.gamma6 * (ps - pr) / pr));
-        const float wl = sqrtf(cl * (1.f + C.gamma6 * (ps - pl) / pl));
+        // Sampling (FP32).  W^2 at p* from the iteration's coefficients, and
+        // 1/W by one reciprocal square root per side (W = W^2 / W).
+        const float wl2 = (float)fma(kl, pst - pld, cld);
+        const float wr2 = (float)fma(kr, pst - prd, crd);
+        const float iwl = rsqrtf(wl2), iwr = rsqrtf(wr2);
+        const float wl = wl2 * iwl, wr = wr2 * iwr;
         // u* grouped as (ul + ur) + (left term - right term): a mirror pair
         // (a reflecting wall: ur = -ul, identical pressures and W) gives
         // u* = 0 exactly, so the wall's mass and energy fluxes vanish
         // exactly.  The reference's order, ul + A_l + ur - A_r, leaves FP32
         // rounding of A, which is large next to near-vacuum states.
-        const float ustar = 0.5f * ((ul + ur) + ((pl - ps) / wl - (pr - ps) / wr));
+        const float ustar = 0.5f * ((ul + ur) + ((pl - ps) * iwl - (pr - ps) * iwr));
         const bool left = ustar > 0.f;
         const float sgnm = left ? 1.f : -1.f;
         const float ro = left ? rl : rr, uo = left ? ul : ur, po = left ? pl : pr;
         const float wo = left ? wl : wr;
+        const float iwo = left ? iwl : iwr;
         const float iro = 1.0f / ro;
         const float co = fmaxf(C.smallc, sqrtf(fabsf(C.gamma * po * iro)));
-        const float rstar = fmaxf(ro / (1.f + ro * (po - ps) / (wo * wo)), C.smallr * a);
-        const float cstar = fmaxf(C.smallc, sqrtf(fabsf(C.gamma * ps / rstar)));
-        float spout = co - sgnm * uo;
-        float spin = cstar - sgnm * ustar;
-        const float ushock = wo * iro - sgnm * uo;
+        const float den = fmaf(ro * (po - ps), iwo * iwo, 1.f);
+        const float rstar_raw = ro / den;
+        const float rstar = fmaxf(rstar_raw, C.smallr * a);
+        float irs = den * iro;  // 1 / rho* = den / rho_o, unless the floor applies
+        if (rstar != rstar_raw) irs = 1.0f / rstar;
+        const float cstar = fmaxf(C.smallc, sqrtf(fabsf(C.gamma * ps * irs)));
+        float spout = fmaf(-sgnm, uo, co);
+        float spin = fmaf(-sgnm, ustar, cstar);
+        const float ushock = fmaf(wo, iro, -sgnm * uo);
         if (ps >= po) {
             spin = ushock;
             spout = ushock;
         }
         const float scr = fmaxf(spout - spin, C.smallc + fabsf(spout + spin));
-        const float frac = fmaxf(0.f, fminf(1.f, (1.f + (spout + spin) / scr) * 0.5f));
+        const float frac = fmaxf(0.f, fminf(1.f, fmaf((spout + spin) / scr, 0.5f, 0.5f)));
         float gr, gu, gp;
         if (spout < 0.f) {
             gr = ro;
@@ -231,15 +268,15 @@ struct MixedStages {
             gu = ustar;
             gp = ps;
         } else {
-            gr = frac * rstar + (1.f - frac) * ro;
-            gu = frac * ustar + (1.f - frac) * uo;
-            gp = frac * ps + (1.f - frac) * po;
+            gr = fmaf(frac, rstar, (1.f - frac) * ro);
+            gu = fmaf(frac, ustar, (1.f - frac) * uo);
+            gp = fmaf(frac, ps, (1.f - frac) * po);
         }
         const float gv = left ? ql.v : qr.v;
         const float mass = gr * gu;
-        const float ekin = 0.5f * gr * (gu * gu + gv * gv);
-        const float etot = gp * C.entho + ekin;
-        const FluxF f{mass, mass * gu + gp, mass * gv, gu * (etot + gp)};
+        const float ekin = 0.5f * gr * fmaf(gu, gu, gv * gv);
+        const float etot = fmaf(gp, C.entho, ekin);
+        const FluxF f{mass, fmaf(mass, gu, gp), mass * gv, gu * (etot + gp)};
         Flux out{(double)f.d, (double)f.mn, (double)f.mt, (double)f.e};
         if (a != 1.f) {
             const double ia = 1.0 / (double)a;  // a power of two: exact
@@ -266,7 +303,7 @@ struct MixedStages {
         const double r = u.d > C.smallrd ? u.d : C.smallrd;
         const double ir = rcp64(r);
         const double un = u.mn * ir, ut = u.mt * ir;
-        const double e = u.e * ir - 0.5 * (un * un + ut * ut);
+        const double e = fma(u.e, ir, -0.5 * fma(un, un, ut * ut));
         double p = C.gm1d * r * e;
         p = p > r * C.smallpd ? p : r * C.smallpd;
         const double c2 = C.gammad * p * ir;

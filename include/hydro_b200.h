@@ -337,9 +337,12 @@ long long hydro_b200_batch_global_step(hb_batch *b);
 long long hydro_b200_batch_launch_count(hb_batch *b);
 void *hydro_b200_batch_stream(hb_batch *b);
 /* Tiling of the work items: y-segment length, items per queue claim,
- * persistent CTAs per SM (0 = occupancy limit).  Results do not depend on it. */
-int hydro_b200_batch_set_tuning(hb_batch *b, int seg, int claim, int blocks_per_sm);
-int hydro_b200_batch_get_tuning(hb_batch *b, int *seg, int *claim, int *blocks_per_sm);
+ * persistent CTAs per SM (0 = occupancy limit), threads per CTA (64 or 128:
+ * the columns of a y item; an x item's 8 windows are shared by the CTA's
+ * warps).  Results do not depend on it. */
+int hydro_b200_batch_set_tuning(hb_batch *b, int seg, int claim, int blocks_per_sm, int threads);
+int hydro_b200_batch_get_tuning(hb_batch *b, int *seg, int *claim, int *blocks_per_sm,
+                                int *threads);
 /* Times `steps` real global steps per candidate tiling and keeps the fastest
  * (cached per mix of grid shapes).  Returns the global steps advanced. */
 int hydro_b200_batch_autotune(hb_batch *b, int steps);

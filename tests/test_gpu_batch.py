@@ -30,9 +30,14 @@ def mix_of(n, seed, lo=24, hi=200):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_batch_instances_equal_their_single_runs(product_lib, precision):
+@pytest.mark.parametrize("threads", [64, 128])
+def test_batch_instances_equal_their_single_runs(product_lib, precision, threads):
+    """Every instance equals its single-domain run bit for bit, for either CTA
+    size of the item kernels (their register caps differ from the
+    single-grid kernels')."""
     inst = mix_of(7, 11) + [(make_params(37, 29, testcase=1), init_state(make_params(37, 29), 1))]
     b = Batch(inst[0][0], capacity=16, arena_bytes=ARENA, precision=precision)
+    b.set_tuning(64, 4, 0, threads)
     slots = [b.add(H, u) for H, u in inst]
     b.steps(30)
     for s, (H, u0) in zip(slots, inst):
@@ -63,14 +68,15 @@ def test_per_instance_tend(product_lib):
 
 def test_alone_and_in_mix_and_any_tiling(product_lib):
     """Mixed precision: an instance's result does not depend on its company,
-    the queue order, the tiling or the autotuner."""
+    the queue order, the tiling (threads per CTA included) or the autotuner."""
     H, u = blast_instance(160, 96, 0.3, 0.7, 2.0, 1.1)
     solo = Batch(H, capacity=2, arena_bytes=ARENA, precision="mixed")
     s0 = solo.add(H, u)
     solo.steps(24)
     ref = solo.download(s0)
     solo.close()
-    for seg, claim, bps in [(32, 1, 0), (128, 16, 1), (64, 4, 2)]:
+    for seg, claim, bps, threads in [(32, 1, 0, 64), (128, 16, 1, 128), (64, 4, 2, 64),
+                                     (64, 4, 0, 128)]:
         b = Batch(H, capacity=32, arena_bytes=ARENA, precision="mixed")
         others = mix_of(12, seg + claim)
         for Ho, uo in others[:6]:
@@ -78,9 +84,9 @@ def test_alone_and_in_mix_and_any_tiling(product_lib):
         s = b.add(H, u)
         for Ho, uo in others[6:]:
             b.add(Ho, uo)
-        b.set_tuning(seg, claim, bps)
+        b.set_tuning(seg, claim, bps, threads)
         b.steps(24)
-        assert bitwise_equal(b.download(s), ref), (seg, claim, bps)
+        assert bitwise_equal(b.download(s), ref), (seg, claim, bps, threads)
         b.close()
     b = Batch(H, capacity=32, arena_bytes=ARENA, precision="mixed")
     for Ho, uo in mix_of(10, 99):
