@@ -74,20 +74,27 @@ def measured_peak_hbm():
 
 
 def ncu_fp64_pipe():
-    """FP64-pipe utilisation of the two FP64 sweep kernels from the committed
-    ncu summary (percent of peak, x and y sweep), or None."""
+    """FP64-pipe and issue utilisation of the two FP64 sweep kernels at the
+    bench workload, from the committed ncu summary (percent, x and y sweep),
+    or None."""
     import re
-    p = os.path.join(ROOT, "profiles", "sweep_fp64_2048.md")
+    p = os.path.join(ROOT, "profiles", "sweep_fp64_4096.md")
+    out = {}
     try:
         for line in open(p):
-            m = re.match(r"\|\s*FP64 pipe \(%\)\s*\|\s*([0-9.]+)\s*\|\s*([0-9.]+)\s*\|", line)
-            if m:
-                return {"x_sweep": float(m.group(1)), "y_sweep": float(m.group(2)),
-                        "unit": "% of FP64 pipe peak (ncu, 2048² capture)",
-                        "source": "profiles/sweep_fp64_2048.md"}
+            for key, label in (("fp64_pipe_pct", "FP64 pipe (%)"),
+                               ("issue_active_pct", "issue active (%)")):
+                m = re.match(r"\|\s*" + re.escape(label) + r"\s*\|\s*([0-9.]+)\s*\|\s*([0-9.]+)\s*\|",
+                             line)
+                if m:
+                    out[key] = {"x_sweep": float(m.group(1)), "y_sweep": float(m.group(2))}
     except OSError:
-        pass
-    return None
+        return None
+    if not out:
+        return None
+    out["unit"] = "% of peak (ncu, 4096^2 capture of the bench's sweep kernels)"
+    out["source"] = "profiles/sweep_fp64_4096.md"
+    return out
 
 
 def ncu_traffic_per_launch():

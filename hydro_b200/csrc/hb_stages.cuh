@@ -220,12 +220,21 @@ __device__ __forceinline__ Cons riemann_flux(const Phys& P, const Prim& ql, cons
         double pst = pstar;
         double wwl = sqrt_eq(cl * (1.0 + zdiv(gamma6 * (pst - pl), pl)), cl, wl0);
         double wwr = sqrt_eq(cr * (1.0 + zdiv(gamma6 * (pst - pr), pr)), cr, wr0);
-        double swwl = wwl * wwl;
-        double qlw = 2.0 * wwl * swwl / (swwl + cl);
-        double qrw = 2.0 * wwr * (wwr * wwr) / ((wwr * wwr) + cr);
         double usl = ul - zdiv(pst - pl, wwl);
         double usr = ur + zdiv(pst - pr, wwr);
-        double tmp = (qrw * qlw / (qrw + qlw) * (usl - usr));
+        const double dus = usl - usr;
+        double tmp;
+        if (dus == 0.0) {
+            // q_r q_l / (q_r + q_l) is positive and finite (W_K > 0), so the
+            // product with a signed zero is that zero: the step is dus itself,
+            // without the three divisions.
+            tmp = dus;
+        } else {
+            double swwl = wwl * wwl;
+            double qlw = 2.0 * wwl * swwl / (swwl + cl);
+            double qrw = 2.0 * wwr * (wwr * wwr) / ((wwr * wwr) + cr);
+            tmp = (qrw * qlw / (qrw + qlw) * dus);
+        }
         double delp = omax(tmp, (-pst));
         pst += delp;
         double tmp2 = zdiv(delp, pst + P.smallpp);

@@ -151,21 +151,30 @@ struct FastStages {
         // W_K^2 = c_K (1 + gamma6 (p - p_K) / p_K) = c_K + k_K (p - p_K).
         const double kl = cl * P.gamma6 * rcp64(pl);
         const double kr = cr * P.gamma6 * rcp64(pr);
-        double il = rsqrt64(cl), ir = rsqrt64(cr);      // 1 / W at p = p_K
+        const double il0 = rsqrt64(cl), ir0 = rsqrt64(cr);  // 1 / W at p = p_K
+        double il = il0, ir = ir0;
         const double wl0 = cl * il, wr0 = cr * ir;
         double pst = fmax(((wr0 * pl + wl0 * pr) + wl0 * wr0 * (ul - ur)) * rcp64(wl0 + wr0), 0.0);
 
+        // Where p equals p_K, W^2 is c_K and 1/W is known (the usual case
+        // between equal states); a zero velocity jump makes the step zero.
         for (int iter = 0; iter < P.niter; iter++) {
             const double wl2 = fma(kl, pst - pl, cl);
             const double wr2 = fma(kr, pst - pr, cr);
-            il = rsqrt64(wl2);
-            ir = rsqrt64(wr2);
+            il = il0;
+            if (wl2 != cl) il = rsqrt64(wl2);
+            ir = ir0;
+            if (wr2 != cr) ir = rsqrt64(wr2);
             const double usl = ul - (pst - pl) * il;
             const double usr = ur + (pst - pr) * ir;
-            // 1/q_K = (W^2 + c_K) / (2 W^3)
-            const double iql = 0.5 * (wl2 + cl) * (il * il * il);
-            const double iqr = 0.5 * (wr2 + cr) * (ir * ir * ir);
-            double delp = (usl - usr) * rcp64(iql + iqr);
+            const double dus = usl - usr;
+            double delp = 0.0;
+            if (dus != 0.0) {
+                // 1/q_K = (W^2 + c_K) / (2 W^3)
+                const double iql = 0.5 * (wl2 + cl) * (il * il * il);
+                const double iqr = 0.5 * (wr2 + cr) * (ir * ir * ir);
+                delp = dus * rcp64(iql + iqr);
+            }
             delp = delp > -pst ? delp : -pst;
             pst += delp;
             if (!(fabs(delp) > 1e-6 * (pst + P.smallpp))) break;
@@ -174,8 +183,10 @@ struct FastStages {
 
         const double wr2 = fma(kr, pstar - pr, cr);
         const double wl2 = fma(kl, pstar - pl, cl);
-        ir = rsqrt64(wr2);
-        il = rsqrt64(wl2);
+        ir = ir0;
+        if (wr2 != cr) ir = rsqrt64(wr2);
+        il = il0;
+        if (wl2 != cl) il = rsqrt64(wl2);
         const double ustar = 0.5 * (ul + (pl - pstar) * il + ur - (pr - pstar) * ir);
         const bool left = ustar > 0.0;
         const double sgnm = left ? 1.0 : -1.0;
