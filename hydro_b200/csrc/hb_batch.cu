@@ -174,7 +174,7 @@ int build_lists(hb_batch* b) {
         if (b->off[s] < 0 || !I.active) continue;
         const bool even = (I.nstep % 2) == 0;
         const int xl = even ? 0 : 1, yl = 1 - xl;
-        for (int l0 = 0; l0 < I.nx; l0 += b->tune.threads)
+        for (int l0 = 0; l0 < I.nx; l0 += hb::kBatchYItemColumns)
             for (int k0 = 2; k0 < I.ny + 2; k0 += b->tune.seg)
                 L[yl][1].push_back(WorkItem{s, 2, l0, k0});
         // x windows of the stage set's width (two cells per lane in mixed precision)

@@ -39,38 +39,43 @@ __device__ __forceinline__ SweepArgs batch_args(const BatchInst& I, int dir, int
     return a;
 }
 
-// Persistent CTAs claim `claim` items at a time until the list is exhausted;
-// every item of the list sweeps direction DIR (x: cell-per-lane windows of a
-// row, y: marching groups of T columns), so each direction has its own kernel
-// with its own register budget.  An item's instance is skipped once its clock
-// has stopped.  The second sweep of an instance's odd step also reduces its
-// Courant maxima.
+// Persistent CTAs claim items until the list is exhausted; every item of the
+// list sweeps direction DIR, so each direction has its own kernel with its own
+// register budget.  An x item (cell-per-lane windows of a row) is shared by the
+// CTA's warps, which claims `claim` of them at a time; a y item (a marching
+// group of 32 columns) belongs to one warp, and the CTA claims `claim` per warp.
+// An item's instance is skipped once its clock has stopped.  The second sweep
+// of an instance's odd step also reduces its Courant maxima.
 template <class S, int DIR, int T>
 __device__ __forceinline__ void batch_sweep_body(const BatchLaunch& L, const Phys& P) {
     __shared__ int s_base;
     const typename S::Consts C = S::consts(P);
+    constexpr int kWarps = T / 32;
+    const int warp = threadIdx.x >> 5;
+    const int per_claim = DIR == 1 ? L.claim : L.claim * kWarps;
     for (;;) {
-        if (threadIdx.x == 0) s_base = (int)atomicAdd(L.counter, (unsigned)L.claim);
+        if (threadIdx.x == 0) s_base = (int)atomicAdd(L.counter, (unsigned)per_claim);
         __syncthreads();
         const int base = s_base;
         __syncthreads();
         if (base >= L.nitems) break;
-        const int end = min(base + L.claim, L.nitems);
-        for (int it = base; it < end; it++) {
+        const int end = min(base + per_claim, L.nitems);
+        const int first = DIR == 1 ? base : base + warp;
+        const int stride = DIR == 1 ? 1 : kWarps;
+        for (int it = first; it < end; it += stride) {
             const WorkItem w = L.items[it];
             BatchInst* Ip = L.inst + w.slot;
             const BatchInst I = *Ip;
-            if (!I.active) continue;  // CTA-uniform
+            if (!I.active) continue;  // uniform over the item's threads
             const bool fuse = (L.phase == 2) && (I.nstep & 1);
             const SweepArgs a = batch_args(I, DIR, L.phase, fuse, Ip);
             const double dtdx = I.dt / I.dx;
             double cx = 0.0, cy = 0.0;
             if (DIR == 1) {
-                const int warp = threadIdx.x >> 5;
-                for (int win = w.k0 + warp; win < w.k0 + kXItemWindows; win += T / 32)
+                for (int win = w.k0 + warp; win < w.k0 + kXItemWindows; win += kWarps)
                     xcell_window<S>(a, C, w.line, win, dtdx, cx, cy);
             } else {
-                const int l = w.line + threadIdx.x;
+                const int l = w.line + (threadIdx.x & 31);
                 if (l < a.nlines) {
                     const LineGeom<2> g(a, l);
                     const int k1 = min(w.k0 + L.seg, a.n - 2);

@@ -66,9 +66,9 @@ __device__ __forceinline__ double zdiv(double a, double b) {
 }
 
 // sqrt(x) for an x that often equals x0 > 0 whose square root r0 is already
-// known (a Riemann problem between equal states evaluates W = sqrt(c (1 + 0))
-// four times with the c of its first guess): x == x0 means the same bits, so
-// r0 is sqrt(x) exactly.
+// known (a Riemann problem between equal states has c_r == c_l, and evaluates
+// W = sqrt(c (1 + 0)) four times with the c of its first guess): x == x0 means
+// the same bits, so r0 is sqrt(x) exactly.
 __device__ __forceinline__ double sqrt_eq(double x, double x0, double r0) {
     if (x == x0) return r0;
     return sqrt(x);
@@ -212,7 +212,7 @@ __device__ __forceinline__ Cons riemann_flux(const Phys& P, const Prim& ql, cons
     double cl = gamma * pl * rl;
     double cr = gamma * pr * rr;
     double wl = sqrt(cl);
-    double wr = sqrt(cr);
+    double wr = sqrt_eq(cr, cl, wl);  // equal states: cr == cl
     const double wl0 = wl, wr0 = wr;  // sqrt(cl), sqrt(cr)
     double pstar = cfmax(((wr * pl + wl * pr) + wl * wr * (ul - ur)) / (wl + wr), 0.0);
 
