@@ -176,13 +176,21 @@ int build_lists(hb_batch* b) {
         const int xl = even ? 0 : 1, yl = 1 - xl;
         for (int l0 = 0; l0 < I.nx; l0 += hb::kBatchYItemColumns)
             for (int k0 = 2; k0 < I.ny + 2; k0 += b->tune.seg)
-                L[yl][1].push_back(WorkItem{s, 2, l0, k0});
+                L[yl][1].push_back(WorkItem{s, 2, l0, k0, 1, 0});
         // x windows of the stage set's width (two cells per lane in mixed precision)
         const int wout = b->precision == HB_PREC_MIXED ? hb::kCellWarpOut2 : hb::kCellWarpOut;
         const int nwin = (I.nx + 2 + wout - 1) / wout;
-        for (int l = 0; l < I.ny; l++)
-            for (int w0 = 0; w0 < nwin; w0 += hb::kXItemWindows)
-                L[xl][0].push_back(WorkItem{s, 1, l, w0});
+        if (nwin >= hb::kXItemWindows) {
+            for (int l = 0; l < I.ny; l++)
+                for (int w0 = 0; w0 < nwin; w0 += hb::kXItemWindows)
+                    L[xl][0].push_back(
+                        WorkItem{s, 1, l, w0, 1, std::min(hb::kXItemWindows, nwin - w0)});
+        } else {
+            // A narrow grid: whole rows, as many as make up an item's windows.
+            const int rows = hb::kXItemWindows / nwin;
+            for (int l = 0; l < I.ny; l += rows)
+                L[xl][0].push_back(WorkItem{s, 1, l, 0, std::min(rows, I.ny - l), nwin});
+        }
     }
     for (int w = 0; w < 2; w++)
         for (int d = 0; d < 2; d++) {

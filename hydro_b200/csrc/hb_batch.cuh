@@ -6,10 +6,11 @@
 // every active instance by one time step of its own (main.c:344-408 per
 // instance): a clock kernel (dt on even steps, stop test), two persistent
 // sweep launches that pull work items of all instances from a queue, and a
-// clock kernel (t += dt, nstep++).  An x work item is one row's run of cell
-// windows (cell-per-lane x sweep), shared by a CTA's warps; a y item is a group
-// of 32 columns (one per lane of a warp) over one row segment (marching y
-// sweep).  Instances need not share the sweep order: each instance's first sweep is x on its even steps
+// clock kernel (t += dt, nstep++).  Warps claim work items from a queue: an x
+// item is a run of cell windows of one row, or of several rows of a narrow
+// grid (cell-per-lane x sweep); a y item is a group of 32 columns (one per
+// lane) over one row segment (marching y sweep).  Instances need not share the
+// sweep order: each instance's first sweep is x on its even steps
 // and y on its odd ones, so the host builds two item lists from the
 // instances' step parities and the launches alternate them.
 #pragma once
@@ -37,18 +38,25 @@ struct BatchInst {
     long long stop_step;         // global step at which the instance stopped (-1: running)
 };
 
+// One warp's work: an x item is `wins` consecutive cell windows from window
+// k0 of each of `rows` consecutive rows (narrow grids pack several rows into
+// one item); a y item is 32 columns from `line` marching the row segment that
+// starts at output row k0.
 struct WorkItem {
     int slot;
-    int dir;   // 1: x item (row, first window), 2: y item (first column, first row)
-    int line;  // x: interior row l; y: first interior column l of the column group
+    int dir;   // 1: x item, 2: y item
+    int line;  // x: first interior row; y: first interior column of the group
     int k0;    // x: first cell window; y: first output cell (row) of the segment
+    int rows;  // x: rows of the item (1 for y)
+    int wins;  // x: windows per row (0 for y)
 };
 
 // Threads per CTA of the batched sweep (the autotuner's "threads per tile"):
-// 64 or 128.  An x item's windows are shared by the CTA's warps; a y item is a
-// group of kBatchYItemColumns columns over one row segment, one per lane of a
-// warp.  Narrow grids waste fewer lanes with 32-column groups: on the seeded
-// 256-instance mix (sides 64..1024) 3.1% of y lanes idle, against 8.0% with 64.
+// 64 or 128.  Each warp of a CTA claims its own items, so no CTA barrier sits
+// between items; a y item is a group of kBatchYItemColumns columns over one
+// row segment, one per lane.  Narrow grids waste fewer lanes with 32-column
+// groups: on the seeded 256-instance mix (sides 64..1024) 3.1% of y lanes
+// idle, against 8.0% with 64.
 constexpr int kBatchThreadChoices[2] = {64, 128};
 constexpr int kBatchYItemColumns = 32;
 constexpr int kBatchCourSlots = 16; // Courant accumulator slots per instance
@@ -70,7 +78,7 @@ constexpr int kBatchXThreadsPerSm = 896;
 constexpr int kBatchYThreadsPerSm = 1024;
 constexpr int kBatchXMixedThreadsPerSm = 768;
 constexpr int kBatchYMixedThreadsPerSm = 448;
-constexpr int kXItemWindows = 8;    // cell windows per x item (4 per warp)
+constexpr int kXItemWindows = 4;    // cell windows per x item (one warp's)
 
 struct BatchLaunch {
     BatchInst* inst;
@@ -79,7 +87,7 @@ struct BatchLaunch {
     int phase;                 // 1: A -> B (first sweep of the step), 2: B -> A
     unsigned int* counter;     // claim counter, zero before the launch
     int seg;                   // y-segment length used to build the items
-    int claim;                 // items claimed per atomic
+    int claim;                 // items a warp claims per atomic
     int threads;               // threads per CTA (one of kBatchThreadChoices)
 };
 

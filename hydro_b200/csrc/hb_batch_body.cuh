@@ -39,51 +39,46 @@ __device__ __forceinline__ SweepArgs batch_args(const BatchInst& I, int dir, int
     return a;
 }
 
-// Persistent CTAs claim items until the list is exhausted; every item of the
-// list sweeps direction DIR, so each direction has its own kernel with its own
-// register budget.  An x item (cell-per-lane windows of a row) is shared by the
-// CTA's warps, which claims `claim` of them at a time; a y item (a marching
-// group of 32 columns) belongs to one warp, and the CTA claims `claim` per warp.
-// An item's instance is skipped once its clock has stopped.  The second sweep
-// of an instance's odd step also reduces its Courant maxima.
+// Persistent warps claim `claim` items at a time (lane 0 takes them with one
+// atomic and broadcasts the base) until the list is exhausted, so warps never
+// wait for each other.  Every item of the list sweeps direction DIR, so each
+// direction has its own kernel with its own register budget.  An item's
+// instance is skipped once its clock has stopped.  The second sweep of an
+// instance's odd step also reduces its Courant maxima.
 template <class S, int DIR, int T>
 __device__ __forceinline__ void batch_sweep_body(const BatchLaunch& L, const Phys& P) {
-    __shared__ int s_base;
     const typename S::Consts C = S::consts(P);
-    constexpr int kWarps = T / 32;
-    const int warp = threadIdx.x >> 5;
-    const int per_claim = DIR == 1 ? L.claim : L.claim * kWarps;
+    const int lane = threadIdx.x & 31;
+    const int gwarp = blockIdx.x * (T / 32) + (threadIdx.x >> 5);
     for (;;) {
-        if (threadIdx.x == 0) s_base = (int)atomicAdd(L.counter, (unsigned)per_claim);
-        __syncthreads();
-        const int base = s_base;
-        __syncthreads();
+        int base = 0;
+        if (lane == 0) base = (int)atomicAdd(L.counter, (unsigned)L.claim);
+        base = __shfl_sync(0xffffffffu, base, 0);
         if (base >= L.nitems) break;
-        const int end = min(base + per_claim, L.nitems);
-        const int first = DIR == 1 ? base : base + warp;
-        const int stride = DIR == 1 ? 1 : kWarps;
-        for (int it = first; it < end; it += stride) {
+        const int end = min(base + L.claim, L.nitems);
+        for (int it = base; it < end; it++) {
             const WorkItem w = L.items[it];
             BatchInst* Ip = L.inst + w.slot;
             const BatchInst I = *Ip;
-            if (!I.active) continue;  // uniform over the item's threads
+            if (!I.active) continue;  // warp-uniform
             const bool fuse = (L.phase == 2) && (I.nstep & 1);
             const SweepArgs a = batch_args(I, DIR, L.phase, fuse, Ip);
             const double dtdx = I.dt / I.dx;
             double cx = 0.0, cy = 0.0;
             if (DIR == 1) {
-                for (int win = w.k0 + warp; win < w.k0 + kXItemWindows; win += kWarps)
-                    xcell_window<S>(a, C, w.line, win, dtdx, cx, cy);
+                for (int r = 0; r < w.rows; r++)
+                    for (int j = 0; j < w.wins; j++)
+                        xcell_window<S>(a, C, w.line + r, w.k0 + j, dtdx, cx, cy);
             } else {
-                const int l = w.line + (threadIdx.x & 31);
+                const int l = w.line + lane;
                 if (l < a.nlines) {
                     const LineGeom<2> g(a, l);
                     const int k1 = min(w.k0 + L.seg, a.n - 2);
-                    march<2, S>(a, C, g, w.k0, k1, dtdx, cx, cy);
+                    march<2, S, T>(a, C, g, w.k0, k1, dtdx, cx, cy);
                 }
             }
             if (fuse) {
-                const int slot = blockIdx.x % kBatchCourSlots;
+                const int slot = gwarp % kBatchCourSlots;
                 warp_max_atomic(&Ip->cour[slot], cx);
                 warp_max_atomic(&Ip->cour[kBatchCourSlots + slot], cy);
             }

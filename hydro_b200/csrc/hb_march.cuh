@@ -152,10 +152,43 @@ struct RowRing {
     }
 };
 
+// Column staging of the y sweep for stage sets with S::async_ring.  Each
+// thread copies the next interior cell of its column into its own column of a
+// 4-slot shared-memory ring with cp.async, one iteration ahead, so the load's
+// latency hides behind an iteration of arithmetic without holding registers;
+// cell k-2 of the update is read back from the ring.  Slots hold cells k-2,
+// k-1, k and k+1; the copy of k+1 reuses the slot of k-3, no longer needed.
+// Each thread touches only its own column, so no barrier is needed.
+template <int RW>
+struct ColumnRing {
+    double (*t)[4][RW];  // [variable][ring position][thread]
+    int tid;
+    __device__ __forceinline__ void issue(const SweepArgs& a, const LineGeom<2>& g, int k) {
+        const double* p = a.in + g.at(k);
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+            const unsigned dst = (unsigned)__cvta_generic_to_shared(&t[v][k & 3][tid]);
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst),
+                         "l"(p + v * a.vs)
+                         : "memory");
+        }
+    }
+    __device__ __forceinline__ void commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+    // Every group but the most recent one has landed.
+    __device__ __forceinline__ void wait_all_but_last() {
+        asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+    }
+    __device__ __forceinline__ Cons cell(int k) const {
+        constexpr int mn = Slots<2>::mn, mt = Slots<2>::mt;
+        return Cons{t[0][k & 3][tid], t[mn][k & 3][tid], t[mt][k & 3][tid], t[3][k & 3][tid]};
+    }
+};
+
 // The march of one thread over [k0, k1); S::Prim / S::Flux are the stage set's
 // primitive and flux records, S::Sound what its primitives step hands to its
 // trace step (the sound speed, with reciprocals in the mixed set).
-template <int DIR, class S>
+// RW: threads of the CTA (the width of the y sweep's column ring).
+template <int DIR, class S, int RW = kSweepThreads>
 __device__ __forceinline__ void march(const SweepArgs& a, const typename S::Consts& C,
                                       const LineGeom<DIR>& g, int k0, int k1, double dtdx,
                                       double& cx, double& cy) {
@@ -179,15 +212,29 @@ __device__ __forceinline__ void march(const SweepArgs& a, const typename S::Cons
     Flux fprev = S::zero_flux();                    // flux at (k-3 | k-2)
 
     // y sweep of a stage set with S::prefetch: the next cell is loaded one
-    // iteration ahead, so its latency hides behind this iteration's
-    // arithmetic (costs registers; the FP64 set, bound by arithmetic, keeps
-    // its occupancy instead).
+    // iteration ahead into registers, so its latency hides behind this
+    // iteration's arithmetic.  With S::async_ring it is copied ahead into the
+    // shared-memory column ring instead, which costs no registers.
     constexpr bool pre = DIR == 2 && S::prefetch;
+    constexpr bool aring = DIR == 2 && !pre && S::async_ring;
+    __shared__ double col_mem[aring ? 4 : 1][4][aring ? RW : 1];
+    ColumnRing<aring ? RW : 1> col{col_mem, (int)threadIdx.x};
+    if (aring) {
+        if (k0 - 2 >= 2) col.issue(a, reinterpret_cast<const LineGeom<2>&>(g), k0 - 2);
+        col.commit();
+    }
     Cons next = pre ? load_cell<DIR>(a, g, k0 - 2) : Cons{0.0, 0.0, 0.0, 0.0};
     for (int k = k0 - 2; k <= k1 + 1; k++) {
         Cons uk;
         Cons u2{0.0, 0.0, 0.0, 0.0};
-        if (DIR == 1) {
+        if (aring) {
+            const int kn = k + 1;  // interior cells only; ghosts take the fused fill
+            if (kn <= k1 + 1 && kn >= 2 && kn < a.n - 2)
+                col.issue(a, reinterpret_cast<const LineGeom<2>&>(g), kn);
+            col.commit();
+            col.wait_all_but_last();
+            uk = (k >= 2 && k < a.n - 2) ? col.cell(k) : load_cell<DIR>(a, g, k);
+        } else if (DIR == 1) {
             if (((k - (k0 - 2)) & 3) == 0) ring.fill(a, reinterpret_cast<const LineGeom<1>&>(g), k,
                                                      k1 + 1, vec_ok);
             uk = (k >= 2 && k < a.n - 2) ? ring.cell(k) : load_cell<DIR>(a, g, k);
@@ -214,6 +261,7 @@ __device__ __forceinline__ void march(const SweepArgs& a, const typename S::Cons
                 f = S::riemann(C, xm2, xp1);
                 if (k >= k0 + 2) {
                     if (DIR == 1) u2 = ring.cell(k - 2);
+                    else if (aring) u2 = col.cell(k - 2);
                     else if (!pre) u2 = load_interior<DIR>(a, g, k - 2);
                     const Cons o = S::update(u2, fprev, f, dtdx);
                     store_cell<DIR>(a, g, k - 2, o);

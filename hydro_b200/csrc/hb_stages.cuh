@@ -331,6 +331,7 @@ struct ExactStages {
     using Sound = double;  // the sound speed, from prim to trace
     using TraceK = hb::TraceK;
     static constexpr bool prefetch = false;
+    static constexpr bool async_ring = false;  // the y march stages cells by cp.async
     static constexpr int cells_per_lane = 1;  // x sweep window (hb_march.cuh)
     static __device__ __forceinline__ Consts consts(const Phys& P) { return P; }
     static __device__ __forceinline__ Prim zero_prim() { return Prim{0.0, 0.0, 0.0, 0.0}; }

@@ -45,6 +45,7 @@ struct FastStages {
     using Sound = double;  // the sound speed, from prim to trace
     using TraceK = hb::TraceK;
     static constexpr bool prefetch = false;
+    static constexpr bool async_ring = false;  // the y march stages cells by cp.async
     static constexpr int cells_per_lane = 1;
 
     static __device__ __forceinline__ Consts consts(const Phys& P) {

@@ -61,6 +61,7 @@ struct MixedStages {
     using Sound = SoundF;
     using TraceK = TraceKF;
     static constexpr bool prefetch = true;
+    static constexpr bool async_ring = false;  // the y march prefetches into registers
     static constexpr int cells_per_lane = 2;  // x sweep window (hb_march.cuh)
 
     static __device__ __forceinline__ Consts consts(const Phys& P) {
