@@ -68,7 +68,7 @@ constexpr int kBatchCourSlots = 16; // Courant accumulator slots per instance
 //  - FP64 y items: 1024, the plain FP64 march's cap (64 registers): 134
 //    registers uncapped, 15% slower per batched step.
 //  - mixed x items: 768 (80 registers), the plain mixed x sweep's.
-//  - mixed y items (marching, prefetching): 448; uncapped they take 147
+//  - mixed y items (marching, cp.async column ring): 448; uncapped they take 147
 //    registers (6 CTAs of 64), 7 CTAs of 64 are 3% faster, 8 less so.
 // The caps need not match the single-grid kernels': no stage set rounds
 // differently in another kernel (the FP64 set rounds every operation once,

@@ -74,9 +74,9 @@ constexpr int kCellThreads = 64;
 // caps).  The FP64 kernels are latency-bound: more resident warps beat the
 // few register spills the caps cause (measured at 4096^2: marching y sweep
 // 1.66 -> 1.49 ms, cell-per-lane x sweep 1.63 -> 1.56 ms).  The mixed marching
-// sweep keeps its registers for the next-cell prefetch and is not capped; the
-// mixed x sweep (two cells per lane) runs best at 12 CTAs per SM (80
-// registers): 0.419 ms at 4096^2, against 0.477 ms one cell per lane.
+// sweep is not capped; the mixed x sweep (two cells per lane) runs best at 12
+// CTAs per SM (80 registers): 0.419 ms at 4096^2, against 0.477 ms one cell
+// per lane.
 constexpr int kFp64MarchMinBlocks = 16;
 constexpr int kFp64CellMinBlocks = 18;
 constexpr int kMixedCellMinBlocks = 12;

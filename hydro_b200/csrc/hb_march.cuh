@@ -211,19 +211,16 @@ __device__ __forceinline__ void march(const SweepArgs& a, const typename S::Cons
     Prim xm2 = S::zero_prim();                      // qxm of k-2
     Flux fprev = S::zero_flux();                    // flux at (k-3 | k-2)
 
-    // y sweep of a stage set with S::prefetch: the next cell is loaded one
-    // iteration ahead into registers, so its latency hides behind this
-    // iteration's arithmetic.  With S::async_ring it is copied ahead into the
-    // shared-memory column ring instead, which costs no registers.
-    constexpr bool pre = DIR == 2 && S::prefetch;
-    constexpr bool aring = DIR == 2 && !pre && S::async_ring;
+    // y sweep of a stage set with S::async_ring: the next cell is copied one
+    // iteration ahead into the shared-memory column ring, so its latency hides
+    // behind this iteration's arithmetic without holding registers.
+    constexpr bool aring = DIR == 2 && S::async_ring;
     __shared__ double col_mem[aring ? 4 : 1][4][aring ? RW : 1];
     ColumnRing<aring ? RW : 1> col{col_mem, (int)threadIdx.x};
     if (aring) {
         if (k0 - 2 >= 2) col.issue(a, reinterpret_cast<const LineGeom<2>&>(g), k0 - 2);
         col.commit();
     }
-    Cons next = pre ? load_cell<DIR>(a, g, k0 - 2) : Cons{0.0, 0.0, 0.0, 0.0};
     for (int k = k0 - 2; k <= k1 + 1; k++) {
         Cons uk;
         Cons u2{0.0, 0.0, 0.0, 0.0};
@@ -238,12 +235,6 @@ __device__ __forceinline__ void march(const SweepArgs& a, const typename S::Cons
             if (((k - (k0 - 2)) & 3) == 0) ring.fill(a, reinterpret_cast<const LineGeom<1>&>(g), k,
                                                      k1 + 1, vec_ok);
             uk = (k >= 2 && k < a.n - 2) ? ring.cell(k) : load_cell<DIR>(a, g, k);
-        } else if (pre) {
-            uk = next;
-            if (k <= k1) next = load_cell<DIR>(a, g, k + 1);
-            // Cell k-2, updated in this iteration, is read again (a cache hit)
-            // instead of being carried in registers.
-            if (k >= k0 + 2) u2 = load_interior<DIR>(a, g, k - 2);
         } else {
             uk = load_cell<DIR>(a, g, k);
         }
@@ -262,7 +253,9 @@ __device__ __forceinline__ void march(const SweepArgs& a, const typename S::Cons
                 if (k >= k0 + 2) {
                     if (DIR == 1) u2 = ring.cell(k - 2);
                     else if (aring) u2 = col.cell(k - 2);
-                    else if (!pre) u2 = load_interior<DIR>(a, g, k - 2);
+                    // Otherwise cell k-2 is read again (a cache hit) instead of
+                    // being carried in registers.
+                    else u2 = load_interior<DIR>(a, g, k - 2);
                     const Cons o = S::update(u2, fprev, f, dtdx);
                     store_cell<DIR>(a, g, k - 2, o);
                     if (a.courant) {

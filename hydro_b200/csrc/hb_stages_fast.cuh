@@ -44,8 +44,9 @@ struct FastStages {
     using Real = double;   // element type of Prim
     using Sound = double;  // the sound speed, from prim to trace
     using TraceK = hb::TraceK;
-    static constexpr bool prefetch = false;
-    static constexpr bool async_ring = false;  // the y march stages cells by cp.async
+    // Staging the y march's cells by cp.async (the mixed set's column ring)
+    // measured slower for the FP64 sets (4096^2: 0.791 against 0.760 ms).
+    static constexpr bool async_ring = false;
     static constexpr int cells_per_lane = 1;
 
     static __device__ __forceinline__ Consts consts(const Phys& P) {

@@ -60,8 +60,9 @@ struct MixedStages {
     using Real = float;     // element type of Prim
     using Sound = SoundF;
     using TraceK = TraceKF;
-    static constexpr bool prefetch = true;
-    static constexpr bool async_ring = false;  // the y march prefetches into registers
+    // The y march stages the next cell with cp.async into a shared-memory ring
+    // (4096^2: 0.346 ms per y sweep, against 0.355 ms prefetching into registers).
+    static constexpr bool async_ring = true;
     static constexpr int cells_per_lane = 2;  // x sweep window (hb_march.cuh)
 
     static __device__ __forceinline__ Consts consts(const Phys& P) {
