@@ -45,6 +45,24 @@ def test_mixed_l1_error_against_fp64(product_lib, nx, ny, tc, nsteps, noise):
     assert np.all(np.isfinite(mix))
 
 
+@pytest.mark.parametrize("nx,ny,tc,nsteps", [(250, 125, 1, 100), (300, 220, 0, 120)])
+def test_mixed_l1_error_against_the_oracle(product_lib, oracle, nx, ny, tc, nsteps):
+    """The bound checked directly against the CPU oracle (itself bitwise the
+    reference), not only through the FP64 GPU path."""
+    from _helpers import orc_from_H
+    H = make_params(nx, ny, testcase=tc)
+    p = orc_from_H(oracle, H)
+    want = oracle.init_state(p, tc)
+    u0 = want.copy()
+    n, _, wt = oracle.run(p, want, nsteps)
+    mix, tmix = run(H, u0, nsteps, "mixed")
+    err = field_errors(mix, want)
+    assert n == nsteps
+    assert err["rho"]["l1_rel"] <= L1_BOUND, err
+    assert err["E"]["l1_rel"] <= L1_BOUND, err
+    assert abs(tmix - wt) <= 1e-5 * wt
+
+
 def test_mixed_full_size_noisy_corner_8192(product_lib, capsys):
     """The mixed-precision workload at its full size: 8192^2, corner blast,
     density times 1 + 0.01 U(-1, 1), 500 steps, against the FP64 path on the
