@@ -41,7 +41,7 @@ int fail(int code, const char* what, cudaError_t e = cudaSuccess) {
 
 struct Tuning {
     int seg = 64;          // y-segment length of y items
-    int claim = 4;         // items per claim
+    int claim = 1;         // items a warp claims at a time
     int blocks_per_sm = 0; // persistent CTAs per SM (0: occupancy limit)
     int threads = 64;      // threads per CTA (columns per y item)
 };
