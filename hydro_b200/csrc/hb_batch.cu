@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -18,7 +19,7 @@ int hb_record_error(int code, const char* msg);  // hb_runtime.cu
 
 using hb::BatchInst;
 using hb::BatchLaunch;
-using hb::WorkItem;
+using hb::ItemRun;
 
 namespace {
 
@@ -116,10 +117,12 @@ struct hb_batch {
     Arena arena;
     double* arena_mem = nullptr;
     // work lists: [list][dir-1]; list 0 holds the first sweeps of an
-    // even-parity step, list 1 the second sweeps; one list per direction
-    WorkItem* items_d[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    // even-parity step, list 1 the second sweeps; one list per direction, as
+    // runs of items (ItemRun, at most one per slot) and their first indices
+    ItemRun* runs_d[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    int* first_d[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    int nruns[2][2] = {{0, 0}, {0, 0}};
     int nitems[2][2] = {{0, 0}, {0, 0}};
-    int items_cap[2][2] = {{0, 0}, {0, 0}};
     long long lists_step = -1;       // global step the lists' parities refer to
     bool lists_dirty = true;
     unsigned int* counters = nullptr;  // [2 phases][2 directions]
@@ -154,53 +157,55 @@ int sync_table_up(hb_batch* b) {
     return HB_OK;
 }
 
-int ensure_items(hb_batch* b, int list, int d, int n) {
-    if (n <= b->items_cap[list][d]) return HB_OK;
-    cudaFree(b->items_d[list][d]);
-    b->items_d[list][d] = nullptr;
-    b->items_cap[list][d] = 0;
-    HB_BCU(cudaMalloc(&b->items_d[list][d], sizeof(WorkItem) * (size_t)std::max(n, 1)));
-    b->items_cap[list][d] = n;
-    return HB_OK;
-}
-
 // Lists for the current global step: list 0 holds each active instance's
 // first-sweep items (x on even nstep, y on odd), list 1 its second-sweep
-// items, each split by direction.
+// items, each split by direction.  One run per instance and list (ItemRun).
 int build_lists(hb_batch* b) {
-    std::vector<WorkItem> L[2][2];
+    std::vector<ItemRun> R[2][2];
+    std::vector<int> F[2][2];
+    long long n[2][2] = {{0, 0}, {0, 0}};
+    auto add = [&](int w, int d, const ItemRun& r, long long count) {
+        R[w][d].push_back(r);
+        F[w][d].push_back((int)n[w][d]);
+        n[w][d] += count;
+    };
     for (int s = 0; s < b->capacity; s++) {
         const BatchInst& I = b->h[s];
         if (b->off[s] < 0 || !I.active) continue;
         const bool even = (I.nstep % 2) == 0;
         const int xl = even ? 0 : 1, yl = 1 - xl;
-        for (int l0 = 0; l0 < I.nx; l0 += hb::kBatchYItemColumns)
-            for (int k0 = 2; k0 < I.ny + 2; k0 += b->tune.seg)
-                L[yl][1].push_back(WorkItem{s, 2, l0, k0, 1, 0});
+        const int groups = (I.nx + hb::kBatchYItemColumns - 1) / hb::kBatchYItemColumns;
+        const int segs = (I.ny + b->tune.seg - 1) / b->tune.seg;
+        add(yl, 1, ItemRun{s, segs, 0, 0}, (long long)groups * segs);
         // x windows of the stage set's width (two cells per lane in mixed precision)
         const int wout = b->precision == HB_PREC_MIXED ? hb::kCellWarpOut2 : hb::kCellWarpOut;
         const int nwin = (I.nx + 2 + wout - 1) / wout;
         if (nwin >= hb::kXItemWindows) {
-            for (int l = 0; l < I.ny; l++)
-                for (int w0 = 0; w0 < nwin; w0 += hb::kXItemWindows)
-                    L[xl][0].push_back(
-                        WorkItem{s, 1, l, w0, 1, std::min(hb::kXItemWindows, nwin - w0)});
+            const int per = (nwin + hb::kXItemWindows - 1) / hb::kXItemWindows;
+            add(xl, 0, ItemRun{s, per, nwin, 0}, (long long)I.ny * per);
         } else {
             // A narrow grid: whole rows, as many as make up an item's windows.
             const int rows = hb::kXItemWindows / nwin;
-            for (int l = 0; l < I.ny; l += rows)
-                L[xl][0].push_back(WorkItem{s, 1, l, 0, std::min(rows, I.ny - l), nwin});
+            add(xl, 0, ItemRun{s, -rows, nwin, 0}, (I.ny + rows - 1) / rows);
         }
     }
     for (int w = 0; w < 2; w++)
         for (int d = 0; d < 2; d++) {
-            int rc = ensure_items(b, w, d, (int)L[w][d].size());
-            if (rc) return rc;
-            if (!L[w][d].empty())
-                HB_BCU(cudaMemcpyAsync(b->items_d[w][d], L[w][d].data(),
-                                       sizeof(WorkItem) * L[w][d].size(), cudaMemcpyHostToDevice,
+            if (n[w][d] > INT_MAX) return fail(HB_ERR_ARG, "batch: more than 2^31 work items");
+            if (!b->runs_d[w][d]) {
+                HB_BCU(cudaMalloc(&b->runs_d[w][d], sizeof(ItemRun) * (size_t)b->capacity));
+                HB_BCU(cudaMalloc(&b->first_d[w][d], sizeof(int) * (size_t)b->capacity));
+            }
+            if (!R[w][d].empty()) {
+                HB_BCU(cudaMemcpyAsync(b->runs_d[w][d], R[w][d].data(),
+                                       sizeof(ItemRun) * R[w][d].size(), cudaMemcpyHostToDevice,
                                        b->stream));
-            b->nitems[w][d] = (int)L[w][d].size();
+                HB_BCU(cudaMemcpyAsync(b->first_d[w][d], F[w][d].data(),
+                                       sizeof(int) * F[w][d].size(), cudaMemcpyHostToDevice,
+                                       b->stream));
+            }
+            b->nruns[w][d] = (int)R[w][d].size();
+            b->nitems[w][d] = (int)n[w][d];
         }
     HB_BCU(cudaStreamSynchronize(b->stream));
     b->lists_step = b->gstep;
@@ -222,7 +227,9 @@ int launch_sweep(hb_batch* b, int list, int phase, cudaStream_t s) {
     for (int dir = 1; dir <= 2; dir++) {
         BatchLaunch L;
         L.inst = b->d;
-        L.items = b->items_d[list][dir - 1];
+        L.runs = b->runs_d[list][dir - 1];
+        L.run_first = b->first_d[list][dir - 1];
+        L.nruns = b->nruns[list][dir - 1];
         L.nitems = b->nitems[list][dir - 1];
         L.phase = phase;
         L.counter = b->counters + 2 * (phase - 1) + (dir - 1);
@@ -382,7 +389,10 @@ extern "C" void hydro_b200_batch_destroy(hb_batch* b) {
     for (int f = 0; f < 2; f++)
         if (b->graph[f]) cudaGraphExecDestroy(b->graph[f]);
     for (int w = 0; w < 2; w++)
-        for (int d = 0; d < 2; d++) cudaFree(b->items_d[w][d]);
+        for (int d = 0; d < 2; d++) {
+            cudaFree(b->runs_d[w][d]);
+            cudaFree(b->first_d[w][d]);
+        }
     cudaFree(b->d);
     cudaFree(b->gstep_d);
     cudaFree(b->counters);

@@ -12,7 +12,10 @@
 // lane) over one row segment (marching y sweep).  Instances need not share the
 // sweep order: each instance's first sweep is x on its even steps
 // and y on its odd ones, so the host builds two item lists from the
-// instances' step parities and the launches alternate them.
+// instances' step parities and the launches alternate them.  A list holds no
+// record per item: it is a run per instance (its first item's index and its
+// item counts), and a warp decodes the item it claims from its index, so the
+// host's cost of building a list grows with the instances, not with the cells.
 #pragma once
 
 #include "hb_kernels.cuh"
@@ -44,11 +47,24 @@ struct BatchInst {
 // starts at output row k0.
 struct WorkItem {
     int slot;
-    int dir;   // 1: x item, 2: y item
     int line;  // x: first interior row; y: first interior column of the group
     int k0;    // x: first cell window; y: first output cell (row) of the segment
     int rows;  // x: rows of the item (1 for y)
     int wins;  // x: windows per row (0 for y)
+};
+
+// The items of one instance in one list, numbered from `first` in the list:
+//  - x, a grid of at least kXItemWindows windows per row: `per` items per row,
+//    item j covers row j / per, windows from (j % per) * kXItemWindows;
+//  - x, a narrower grid: per = -(rows per item), item j covers rows from
+//    j * rows, all `nwin` windows of each;
+//  - y: `per` row segments per column group, item j is group j / per
+//    (kBatchYItemColumns columns), segment j % per.
+struct ItemRun {
+    int slot;
+    int per;
+    int nwin;   // x: cell windows per row
+    int pad;
 };
 
 // Threads per CTA of the batched sweep (the autotuner's "threads per tile"):
@@ -82,8 +98,10 @@ constexpr int kXItemWindows = 4;    // cell windows per x item (one warp's)
 
 struct BatchLaunch {
     BatchInst* inst;
-    const WorkItem* items;
-    int nitems;
+    const ItemRun* runs;       // one per instance with items in this list
+    const int* run_first;      // list index of each run's first item (ascending, from 0)
+    int nruns;
+    int nitems;                // items in the list (all runs)
     int phase;                 // 1: A -> B (first sweep of the step), 2: B -> A
     unsigned int* counter;     // claim counter, zero before the launch
     int seg;                   // y-segment length used to build the items

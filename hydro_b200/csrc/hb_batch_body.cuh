@@ -39,6 +39,51 @@ __device__ __forceinline__ SweepArgs batch_args(const BatchInst& I, int dir, int
     return a;
 }
 
+// The run holding list item `it`: the last run whose first item is <= it.
+// The warp searches together, 32 candidates a round (two rounds cover 1024
+// runs); run 0 starts at item 0, so lane 0's candidate always qualifies.
+__device__ __forceinline__ int find_run(const int* first, int nruns, int it, int lane) {
+    int lo = 0, n = nruns;
+    while (n > 1) {
+        const int step = (n + 31) >> 5;
+        const bool ok = lane * step < n && __ldg(first + lo + lane * step) <= it;
+        const int k = 31 - __clz(__ballot_sync(0xffffffffu, ok));
+        lo += k * step;
+        n = min(step, n - k * step);
+    }
+    return lo;
+}
+
+// Item `it` of the list, from its run (ItemRun).  `run` carries the warp's
+// last run from claim to claim: consecutive claims mostly fall in it.
+template <int DIR>
+__device__ __forceinline__ WorkItem decode_item(const BatchLaunch& L, int it, int lane, int& run) {
+    const bool hit = run >= 0 && __ldg(L.run_first + run) <= it &&
+                     (run + 1 == L.nruns || it < __ldg(L.run_first + run + 1));
+    if (!hit) run = find_run(L.run_first, L.nruns, it, lane);
+    const ItemRun R = L.runs[run];
+    const int j = it - __ldg(L.run_first + run);
+    WorkItem w;
+    w.slot = R.slot;
+    if (DIR == 2) {
+        w.line = (j / R.per) * kBatchYItemColumns;
+        w.k0 = 2 + (j % R.per) * L.seg;
+        w.rows = 1;
+        w.wins = 0;
+    } else if (R.per > 0) {
+        w.line = j / R.per;
+        w.k0 = (j % R.per) * kXItemWindows;
+        w.rows = 1;
+        w.wins = min(kXItemWindows, R.nwin - w.k0);
+    } else {
+        w.line = j * -R.per;
+        w.k0 = 0;
+        w.rows = -R.per;   // clipped to the grid's rows by the caller
+        w.wins = R.nwin;
+    }
+    return w;
+}
+
 // Persistent warps claim `claim` items at a time (lane 0 takes them with one
 // atomic and broadcasts the base) until the list is exhausted, so warps never
 // wait for each other.  Every item of the list sweeps direction DIR, so each
@@ -50,6 +95,7 @@ __device__ __forceinline__ void batch_sweep_body(const BatchLaunch& L, const Phy
     const typename S::Consts C = S::consts(P);
     const int lane = threadIdx.x & 31;
     const int gwarp = blockIdx.x * (T / 32) + (threadIdx.x >> 5);
+    int run = -1;
     for (;;) {
         int base = 0;
         if (lane == 0) base = (int)atomicAdd(L.counter, (unsigned)L.claim);
@@ -57,7 +103,7 @@ __device__ __forceinline__ void batch_sweep_body(const BatchLaunch& L, const Phy
         if (base >= L.nitems) break;
         const int end = min(base + L.claim, L.nitems);
         for (int it = base; it < end; it++) {
-            const WorkItem w = L.items[it];
+            const WorkItem w = decode_item<DIR>(L, it, lane, run);
             BatchInst* Ip = L.inst + w.slot;
             const BatchInst I = *Ip;
             if (!I.active) continue;  // warp-uniform
@@ -66,7 +112,8 @@ __device__ __forceinline__ void batch_sweep_body(const BatchLaunch& L, const Phy
             const double dtdx = I.dt / I.dx;
             double cx = 0.0, cy = 0.0;
             if (DIR == 1) {
-                for (int r = 0; r < w.rows; r++)
+                const int rows = min(w.rows, I.ny - w.line);
+                for (int r = 0; r < rows; r++)
                     for (int j = 0; j < w.wins; j++)
                         xcell_window<S>(a, C, w.line + r, w.k0 + j, dtdx, cx, cy);
             } else {

@@ -200,36 +200,47 @@ struct MixedStages {
             cl = C.gamma * pl * rl;
             cr = C.gamma * pr * rr;
         }
-        const float wl0 = sqrtf(cl), wr0 = sqrtf(cr);
-        const float p0 =
-            fmaxf(fmaf(wl0 * wr0, ul - ur, fmaf(wr0, pl, wl0 * pr)) / (wl0 + wr0), 0.f);
+        float ps, wl2, wr2;  // p*, and W^2 on both sides at p*
+        if (pl == pr && ul == ur) {
+            // Equal pressure and velocity on both sides (a state at rest, a
+            // uniform flow or a pure contact): the exact solution is p* = p,
+            // at which every Newton step is exactly zero and W^2 = c.
+            ps = pl;
+            wl2 = cl;
+            wr2 = cr;
+        } else {
+            const float wl0 = sqrtf(cl), wr0 = sqrtf(cr);
+            const float p0 =
+                fmaxf(fmaf(wl0 * wr0, ul - ur, fmaf(wr0, pl, wl0 * pr)) / (wl0 + wr0), 0.f);
 
-        // Newton iteration on p* (FP64): W^2 = c (1 + gamma6 (p - p_K) / p_K),
-        // u*_l = u_l - (p - p_l) / W_l, u*_r = u_r + (p - p_r) / W_r, step
-        // dp = (q_l q_r / (q_l + q_r)) (u*_l - u*_r) with q = 2 W^3 / (W^2 + c).
-        const double pld = pl, prd = pr, cld = cl, crd = cr, uld = ul, urd = ur;
-        const double kl = cld * C.gamma6d * rcp64(pld);
-        const double kr = crd * C.gamma6d * rcp64(prd);
-        double pst = p0;
-        for (int iter = 0; iter < C.niter; iter++) {
-            const double wl2 = fma(kl, pst - pld, cld);
-            const double wr2 = fma(kr, pst - prd, crd);
-            const double il = rsqrt64(wl2), ir = rsqrt64(wr2);
-            const double usl = fma(-(pst - pld), il, uld);
-            const double usr = fma(pst - prd, ir, urd);
-            const double iql = 0.5 * (wl2 + cld) * (il * il * il);
-            const double iqr = 0.5 * (wr2 + crd) * (ir * ir * ir);  // 1 / q = (W^2 + c) / (2 W^3)
-            double delp = (usl - usr) * rcp64(iql + iqr);
-            delp = delp > -pst ? delp : -pst;
-            pst += delp;
-            if (!(fabs(delp) > 1e-6 * fabs(pst + C.smallppd * a))) break;
+            // Newton iteration on p* (FP64): W^2 = c (1 + gamma6 (p - p_K) / p_K),
+            // u*_l = u_l - (p - p_l) / W_l, u*_r = u_r + (p - p_r) / W_r, step
+            // dp = (q_l q_r / (q_l + q_r)) (u*_l - u*_r) with q = 2 W^3 / (W^2 + c).
+            const double pld = pl, prd = pr, cld = cl, crd = cr, uld = ul, urd = ur;
+            const double kl = cld * C.gamma6d * rcp64(pld);
+            const double kr = crd * C.gamma6d * rcp64(prd);
+            double pst = p0;
+            for (int iter = 0; iter < C.niter; iter++) {
+                const double wl2d = fma(kl, pst - pld, cld);
+                const double wr2d = fma(kr, pst - prd, crd);
+                const double il = rsqrt64(wl2d), ir = rsqrt64(wr2d);
+                const double usl = fma(-(pst - pld), il, uld);
+                const double usr = fma(pst - prd, ir, urd);
+                const double iql = 0.5 * (wl2d + cld) * (il * il * il);
+                const double iqr = 0.5 * (wr2d + crd) * (ir * ir * ir);  // 1/q = (W^2+c)/(2W^3)
+                double delp = (usl - usr) * rcp64(iql + iqr);
+                delp = delp > -pst ? delp : -pst;
+                pst += delp;
+                if (!(fabs(delp) > 1e-6 * fabs(pst + C.smallppd * a))) break;
+            }
+            ps = (float)pst;
+            // W^2 at p* from the iteration's coefficients.
+            wl2 = (float)fma(kl, pst - pld, cld);
+            wr2 = (float)fma(kr, pst - prd, crd);
         }
-        const float ps = (float)pst;
 
-        // Sampling (FP32).  W^2 at p* from the iteration's coefficients, and
-        // 1/W by one reciprocal square root per side (W = W^2 / W).
-        const float wl2 = (float)fma(kl, pst - pld, cld);
-        const float wr2 = (float)fma(kr, pst - prd, crd);
+        // Sampling (FP32).  1/W by one reciprocal square root per side
+        // (W = W^2 / W).
         const float iwl = rsqrtf(wl2), iwr = rsqrtf(wr2);
         const float wl = wl2 * iwl, wr = wr2 * iwr;
         // u* grouped as (ul + ur) + (left term - right term): a mirror pair

@@ -201,3 +201,21 @@ def test_full_batched_workload_fp64_sampled_bitwise(product_lib):
         want, _, _ = alone(H, u0, 100, "fp64")
         assert bitwise_equal(b.download(slots[i]), want), (i, H.nx, H.ny)
     b.close()
+
+
+def test_many_instances_decode_their_items(product_lib):
+    """1,100 small FP64 instances (over 1,024 item runs per list, so a warp's
+    search for the run of a claimed item takes three rounds): every instance
+    finishes its steps, and a sample equals its single-grid run bit for bit."""
+    mix = make_blast_mix(1100, 7, side_lo=8, side_hi=48)
+    arena = sum(Batch.bytes_needed(H) for H, _ in mix) + (1 << 20)
+    b = Batch(mix[0][0], capacity=1100, arena_bytes=arena, precision="fp64")
+    slots = [b.add(H, u, nstepmax=12) for H, u in mix]
+    b.steps(14)
+    active, nstep, _ = b.table()
+    assert all(nstep[s] == 12 and not active[s] for s in slots)
+    for i in list(range(0, 1100, 97)) + [1098, 1099]:
+        H, u0 = mix[i]
+        want, _, _ = alone(H, u0, 12, "fp64")
+        assert bitwise_equal(b.download(slots[i]), want), (i, H.nx, H.ny)
+    b.close()
