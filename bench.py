@@ -289,6 +289,43 @@ def run_fma_form(H, u0, K, W, ref_state, ref_dts, pg, device, world):
             "precision": "FP64, FMA contraction, refined reciprocals (HB_PREC_FP64_FMA)"}
 
 
+def run_energy_noise_form(H, K, W, pg, device, world, seed=20261205):
+    """The default workload with the interior total energy scaled by
+    1 + 0.01 U(-1, 1) per cell: every interface then has unequal pressures,
+    so no Riemann problem is trivial and every one iterates.  Times the
+    bit-exact FP64 path and the mixed form over the same steps, with the mixed
+    errors against the FP64 state."""
+    import torch
+    from hydro_b200 import Domain
+    from hydro_b200.params import init_noisy_blast
+    u0 = init_noisy_blast(H, seed, testcase=H.testCase, var=3)
+    out = {"workload": f"{H.nx}x{H.ny} centred blast, interior E x (1 + 0.01 U(-1,1)), "
+                       f"steps 0..{K - 1}"}
+    states = {}
+    for prec in ("fp64", "mixed"):
+        d = Domain(H, precision=prec)
+        d.upload(u0)
+        d.set_clock()
+        d.launch_steps(W)
+        d.synchronize()
+        d.upload(u0)
+        d.set_clock()
+        st = torch.cuda.ExternalStream(d.stream_ptr, device=device)
+        barrier(pg, device)
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record(st)
+        d.launch_steps(K)
+        g1.record(st)
+        g1.synchronize()
+        ms = all_max(pg, g0.elapsed_time(g1), device)
+        states[prec] = d.download()
+        d.close()
+        out[prec] = {"value": round(world * H.nx * H.ny * K / (ms / 1e3) / 1e6, 3),
+                     "unit": "Mcell-updates/s", "ms_per_step": round(ms / K, 4)}
+    out["mixed"]["errors_vs_fp64"] = field_errors(states["mixed"], states["fp64"])
+    return out
+
+
 def run_noalloc_form(device):
     """The allocation-free step against the regular domain step on the same
     grids (CUDA events, fixed dt, 50 steps each after 5 warm-up steps)."""
@@ -684,6 +721,7 @@ def main():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-vtk", action="store_true")
+    ap.add_argument("--no-noise", action="store_true")
     ap.add_argument("--serving-wall", type=float, default=20.0)
     ap.add_argument("--knee-wall", type=float, default=8.0)
     args = ap.parse_args()
@@ -804,6 +842,8 @@ def main():
         del mix_state
 
     ref_state = None
+    if not args.no_noise:
+        forms["energy_noise"] = run_energy_noise_form(H, K, W, pg, device, world)
     if not args.no_noalloc and rank == 0 and world == 1:
         forms["noalloc"] = run_noalloc_form(device)
     if not args.no_vtk and rank == 0 and world == 1:

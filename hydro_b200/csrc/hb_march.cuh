@@ -153,34 +153,39 @@ struct RowRing {
 };
 
 // Column staging of the y sweep for stage sets with S::async_ring.  Each
-// thread copies the next interior cell of its column into its own column of a
-// 4-slot shared-memory ring with cp.async, one iteration ahead, so the load's
-// latency hides behind an iteration of arithmetic without holding registers;
-// cell k-2 of the update is read back from the ring.  Slots hold cells k-2,
-// k-1, k and k+1; the copy of k+1 reuses the slot of k-3, no longer needed.
-// Each thread touches only its own column, so no barrier is needed.
-template <int RW>
+// thread copies the interior cell AHEAD rows ahead of its column into its own
+// column of a shared-memory ring with cp.async, so the load's latency hides
+// behind AHEAD iterations of arithmetic without holding registers; cell k-2
+// of the update is read back from the ring.  Slots hold cells k-2 .. k+AHEAD:
+// 4 slots for AHEAD = 1, 8 up to AHEAD = 5; the copy of k+AHEAD reuses the
+// slot of a cell no longer needed.  Each thread touches only its own column,
+// so no barrier is needed.
+template <int RW, int AHEAD>
 struct ColumnRing {
-    double (*t)[4][RW];  // [variable][ring position][thread]
+    static_assert(AHEAD >= 1 && AHEAD <= 5, "ring depth");
+    static constexpr int kSlots = AHEAD + 3 <= 4 ? 4 : 8;
+    double (*t)[kSlots][RW];  // [variable][ring position][thread]
     int tid;
     __device__ __forceinline__ void issue(const SweepArgs& a, const LineGeom<2>& g, int k) {
         const double* p = a.in + g.at(k);
 #pragma unroll
         for (int v = 0; v < 4; v++) {
-            const unsigned dst = (unsigned)__cvta_generic_to_shared(&t[v][k & 3][tid]);
+            const unsigned dst =
+                (unsigned)__cvta_generic_to_shared(&t[v][k & (kSlots - 1)][tid]);
             asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst),
                          "l"(p + v * a.vs)
                          : "memory");
         }
     }
     __device__ __forceinline__ void commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-    // Every group but the most recent one has landed.
-    __device__ __forceinline__ void wait_all_but_last() {
-        asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+    // Every group but the AHEAD most recent ones has landed.
+    __device__ __forceinline__ void wait_ahead() {
+        asm volatile("cp.async.wait_group %0;\n" ::"n"(AHEAD) : "memory");
     }
     __device__ __forceinline__ Cons cell(int k) const {
         constexpr int mn = Slots<2>::mn, mt = Slots<2>::mt;
-        return Cons{t[0][k & 3][tid], t[mn][k & 3][tid], t[mt][k & 3][tid], t[3][k & 3][tid]};
+        const int q = k & (kSlots - 1);
+        return Cons{t[0][q][tid], t[mn][q][tid], t[mt][q][tid], t[3][q][tid]};
     }
 };
 
@@ -215,21 +220,29 @@ __device__ __forceinline__ void march(const SweepArgs& a, const typename S::Cons
     // iteration ahead into the shared-memory column ring, so its latency hides
     // behind this iteration's arithmetic without holding registers.
     constexpr bool aring = DIR == 2 && S::async_ring;
-    __shared__ double col_mem[aring ? 4 : 1][4][aring ? RW : 1];
-    ColumnRing<aring ? RW : 1> col{col_mem, (int)threadIdx.x};
+    constexpr int ahead = aring ? S::ring_ahead : 1;
+    using Ring = ColumnRing<aring ? RW : 1, ahead>;
+    __shared__ double col_mem[aring ? 4 : 1][Ring::kSlots][aring ? RW : 1];
+    Ring col{col_mem, (int)threadIdx.x};
     if (aring) {
-        if (k0 - 2 >= 2) col.issue(a, reinterpret_cast<const LineGeom<2>&>(g), k0 - 2);
-        col.commit();
+        // Interior cells only (ghosts take the fused fill); one group per row,
+        // empty for the rows not copied, so that the group count stays in step.
+        for (int d = 0; d < ahead; d++) {
+            const int kk = k0 - 2 + d;
+            if (kk >= 2 && kk < a.n - 2 && kk <= k1 + 1)
+                col.issue(a, reinterpret_cast<const LineGeom<2>&>(g), kk);
+            col.commit();
+        }
     }
     for (int k = k0 - 2; k <= k1 + 1; k++) {
         Cons uk;
         Cons u2{0.0, 0.0, 0.0, 0.0};
         if (aring) {
-            const int kn = k + 1;  // interior cells only; ghosts take the fused fill
+            const int kn = k + ahead;
             if (kn <= k1 + 1 && kn >= 2 && kn < a.n - 2)
                 col.issue(a, reinterpret_cast<const LineGeom<2>&>(g), kn);
             col.commit();
-            col.wait_all_but_last();
+            col.wait_ahead();
             uk = (k >= 2 && k < a.n - 2) ? col.cell(k) : load_cell<DIR>(a, g, k);
         } else if (DIR == 1) {
             if (((k - (k0 - 2)) & 3) == 0) ring.fill(a, reinterpret_cast<const LineGeom<1>&>(g), k,

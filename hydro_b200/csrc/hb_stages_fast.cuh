@@ -47,6 +47,7 @@ struct FastStages {
     // Staging the y march's cells by cp.async (the mixed set's column ring)
     // measured slower for the FP64 sets (4096^2: 0.791 against 0.760 ms).
     static constexpr bool async_ring = false;
+    static constexpr int ring_ahead = 1;      // rows the ring copies ahead
     static constexpr int cells_per_lane = 1;
 
     static __device__ __forceinline__ Consts consts(const Phys& P) {

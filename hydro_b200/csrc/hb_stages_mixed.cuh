@@ -63,6 +63,7 @@ struct MixedStages {
     // The y march stages the next cell with cp.async into a shared-memory ring
     // (4096^2: 0.346 ms per y sweep, against 0.355 ms prefetching into registers).
     static constexpr bool async_ring = true;
+    static constexpr int ring_ahead = 1;      // rows the ring copies ahead
     static constexpr int cells_per_lane = 2;  // x sweep window (hb_march.cuh)
 
     static __device__ __forceinline__ Consts consts(const Phys& P) {
@@ -200,14 +201,18 @@ struct MixedStages {
             cl = C.gamma * pl * rl;
             cr = C.gamma * pr * rr;
         }
-        float ps, wl2, wr2;  // p*, and W^2 on both sides at p*
+        float gr, gu, gp, gv;  // the state sampled at the interface
         if (pl == pr && ul == ur) {
             // Equal pressure and velocity on both sides (a state at rest, a
-            // uniform flow or a pure contact): the exact solution is p* = p,
-            // at which every Newton step is exactly zero and W^2 = c.
-            ps = pl;
-            wl2 = cl;
-            wr2 = cr;
+            // uniform flow or a pure contact): the exact solution is p* = p and
+            // u* = u, at which every Newton step is exactly zero, and the
+            // interface samples the upwind side's state (right for u = 0),
+            // whichever of the sampling's branches applies.
+            const bool left = ul > 0.f;
+            gr = left ? rl : rr;
+            gu = ul;
+            gp = pl;
+            gv = left ? ql.v : qr.v;
         } else {
             const float wl0 = sqrtf(cl), wr0 = sqrtf(cr);
             const float p0 =
@@ -233,59 +238,57 @@ struct MixedStages {
                 pst += delp;
                 if (!(fabs(delp) > 1e-6 * fabs(pst + C.smallppd * a))) break;
             }
-            ps = (float)pst;
-            // W^2 at p* from the iteration's coefficients.
-            wl2 = (float)fma(kl, pst - pld, cld);
-            wr2 = (float)fma(kr, pst - prd, crd);
-        }
+            const float ps = (float)pst;
 
-        // Sampling (FP32).  1/W by one reciprocal square root per side
-        // (W = W^2 / W).
-        const float iwl = rsqrtf(wl2), iwr = rsqrtf(wr2);
-        const float wl = wl2 * iwl, wr = wr2 * iwr;
-        // u* grouped as (ul + ur) + (left term - right term): a mirror pair
-        // (a reflecting wall: ur = -ul, identical pressures and W) gives
-        // u* = 0 exactly, so the wall's mass and energy fluxes vanish
-        // exactly.  The reference's order, ul + A_l + ur - A_r, leaves FP32
-        // rounding of A, which is large next to near-vacuum states.
-        const float ustar = 0.5f * ((ul + ur) + ((pl - ps) * iwl - (pr - ps) * iwr));
-        const bool left = ustar > 0.f;
-        const float sgnm = left ? 1.f : -1.f;
-        const float ro = left ? rl : rr, uo = left ? ul : ur, po = left ? pl : pr;
-        const float wo = left ? wl : wr;
-        const float iwo = left ? iwl : iwr;
-        const float iro = 1.0f / ro;
-        const float co = fmaxf(C.smallc, sqrtf(fabsf(C.gamma * po * iro)));
-        const float den = fmaf(ro * (po - ps), iwo * iwo, 1.f);
-        const float rstar_raw = ro / den;
-        const float rstar = fmaxf(rstar_raw, C.smallr * a);
-        float irs = den * iro;  // 1 / rho* = den / rho_o, unless the floor applies
-        if (rstar != rstar_raw) irs = 1.0f / rstar;
-        const float cstar = fmaxf(C.smallc, sqrtf(fabsf(C.gamma * ps * irs)));
-        float spout = fmaf(-sgnm, uo, co);
-        float spin = fmaf(-sgnm, ustar, cstar);
-        const float ushock = fmaf(wo, iro, -sgnm * uo);
-        if (ps >= po) {
-            spin = ushock;
-            spout = ushock;
+            // Sampling (FP32).  W^2 at p* from the iteration's coefficients, and
+            // 1/W by one reciprocal square root per side (W = W^2 / W).
+            const float wl2 = (float)fma(kl, pst - pld, cld);
+            const float wr2 = (float)fma(kr, pst - prd, crd);
+            const float iwl = rsqrtf(wl2), iwr = rsqrtf(wr2);
+            const float wl = wl2 * iwl, wr = wr2 * iwr;
+            // u* grouped as (ul + ur) + (left term - right term): a mirror pair
+            // (a reflecting wall: ur = -ul, identical pressures and W) gives
+            // u* = 0 exactly, so the wall's mass and energy fluxes vanish
+            // exactly.  The reference's order, ul + A_l + ur - A_r, leaves FP32
+            // rounding of A, which is large next to near-vacuum states.
+            const float ustar = 0.5f * ((ul + ur) + ((pl - ps) * iwl - (pr - ps) * iwr));
+            const bool left = ustar > 0.f;
+            const float sgnm = left ? 1.f : -1.f;
+            const float ro = left ? rl : rr, uo = left ? ul : ur, po = left ? pl : pr;
+            const float wo = left ? wl : wr;
+            const float iwo = left ? iwl : iwr;
+            const float iro = 1.0f / ro;
+            const float co = fmaxf(C.smallc, sqrtf(fabsf(C.gamma * po * iro)));
+            const float den = fmaf(ro * (po - ps), iwo * iwo, 1.f);
+            const float rstar_raw = ro / den;
+            const float rstar = fmaxf(rstar_raw, C.smallr * a);
+            float irs = den * iro;  // 1 / rho* = den / rho_o, unless the floor applies
+            if (rstar != rstar_raw) irs = 1.0f / rstar;
+            const float cstar = fmaxf(C.smallc, sqrtf(fabsf(C.gamma * ps * irs)));
+            float spout = fmaf(-sgnm, uo, co);
+            float spin = fmaf(-sgnm, ustar, cstar);
+            const float ushock = fmaf(wo, iro, -sgnm * uo);
+            if (ps >= po) {
+                spin = ushock;
+                spout = ushock;
+            }
+            const float scr = fmaxf(spout - spin, C.smallc + fabsf(spout + spin));
+            const float frac = fmaxf(0.f, fminf(1.f, fmaf((spout + spin) / scr, 0.5f, 0.5f)));
+            if (spout < 0.f) {
+                gr = ro;
+                gu = uo;
+                gp = po;
+            } else if (spin > 0.f) {
+                gr = rstar;
+                gu = ustar;
+                gp = ps;
+            } else {
+                gr = fmaf(frac, rstar, (1.f - frac) * ro);
+                gu = fmaf(frac, ustar, (1.f - frac) * uo);
+                gp = fmaf(frac, ps, (1.f - frac) * po);
+            }
+            gv = left ? ql.v : qr.v;
         }
-        const float scr = fmaxf(spout - spin, C.smallc + fabsf(spout + spin));
-        const float frac = fmaxf(0.f, fminf(1.f, fmaf((spout + spin) / scr, 0.5f, 0.5f)));
-        float gr, gu, gp;
-        if (spout < 0.f) {
-            gr = ro;
-            gu = uo;
-            gp = po;
-        } else if (spin > 0.f) {
-            gr = rstar;
-            gu = ustar;
-            gp = ps;
-        } else {
-            gr = fmaf(frac, rstar, (1.f - frac) * ro);
-            gu = fmaf(frac, ustar, (1.f - frac) * uo);
-            gp = fmaf(frac, ps, (1.f - frac) * po);
-        }
-        const float gv = left ? ql.v : qr.v;
         const float mass = gr * gu;
         const float ekin = 0.5f * gr * fmaf(gu, gu, gv * gv);
         const float etot = fmaf(gp, C.entho, ekin);

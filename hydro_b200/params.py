@@ -194,13 +194,15 @@ def uniform_pm1(seed: int, counters: np.ndarray) -> np.ndarray:
     return 2.0 * u - 1.0
 
 
-def init_noisy_blast(H: HydroParam, seed: int, amplitude: float = 0.01, testcase: int = 1):
-    """The test-case state with the interior density scaled by
-    1 + amplitude * U(-1, 1), U drawn per interior cell (counter = j*nx + i,
-    interior coordinates) -- the mixed-precision workload's input."""
+def init_noisy_blast(H: HydroParam, seed: int, amplitude: float = 0.01, testcase: int = 1,
+                     var: int = 0):
+    """The test-case state with the interior of conserved variable `var`
+    (0: density -- the mixed-precision workload's input; 3: total energy)
+    scaled by 1 + amplitude * U(-1, 1), U drawn per interior cell
+    (counter = j*nx + i, interior coordinates)."""
     u = init_state(H, testcase)
     j, i = np.meshgrid(np.arange(H.ny, dtype=np.uint64), np.arange(H.nx, dtype=np.uint64),
                        indexing="ij")
     noise = uniform_pm1(seed, j * np.uint64(H.nx) + i)
-    u[0, 2:-2, 2:-2] *= 1.0 + amplitude * noise
+    u[var, 2:-2, 2:-2] *= 1.0 + amplitude * noise
     return u

@@ -144,3 +144,34 @@ def test_mixed_beside_reference_fp32_build(product_lib, capsys, nx, ny, tc, nste
         print(f"\n{nx}x{ny}: mixed vs fp64 {e_mix}\n{nx}x{ny}: reference FP32 build vs fp64 {e_sp}")
     for e in (e_mix, e_sp):
         assert e["rho"]["l1_rel"] <= L1_BOUND and e["E"]["l1_rel"] <= L1_BOUND, (e_mix, e_sp)
+
+
+@pytest.mark.parametrize("vel", [0.0, 0.3])
+def test_mixed_contact_with_equal_pressure_and_velocity(product_lib, vel):
+    """A density step across the grid at uniform pressure and x velocity: every
+    x interface is a trivial Riemann problem (a pure contact), whose exact star
+    state is p* = p, u* = u.  At rest the state must stay exactly unchanged;
+    moving, the momentum and energy stay within rounding of their initial
+    values' ratio to the density (a contact advects without pressure waves)
+    and the result matches the FP64 path to the mixed bound."""
+    H = make_params(256, 64, testcase=0)
+    u0 = init_state(H, 0)
+    rho = np.where(np.arange(H.nx + 4) < (H.nx + 4) // 2, 1.0, 0.125)[None, :]
+    u0[0] = rho
+    u0[1] = rho * vel
+    u0[2] = 0.0
+    p = 1.0
+    u0[3] = p / (H.gamma - 1.0) + 0.5 * rho * vel * vel
+    nsteps = 40
+    mix, _ = run(H, u0, nsteps, "mixed")
+    if vel == 0.0:
+        assert np.array_equal(mix, u0)
+    else:
+        ref, _ = run(H, u0, nsteps, "fp64")
+        err = field_errors(mix, ref)
+        assert err["rho"]["l1_rel"] <= L1_BOUND, err
+        inner = (slice(None), slice(2, -2), slice(56, -56))  # beyond the walls' waves
+        m = mix[inner]
+        assert np.allclose(m[1] / m[0], vel, rtol=0, atol=1e-5)
+        pm = (H.gamma - 1.0) * (m[3] - 0.5 * m[1] ** 2 / m[0])
+        assert np.allclose(pm, p, rtol=1e-5, atol=0)
