@@ -93,6 +93,11 @@ constexpr int kBatchCourSlots = 16; // Courant accumulator slots per instance
 constexpr int kBatchXThreadsPerSm = 896;
 constexpr int kBatchYThreadsPerSm = 1024;
 constexpr int kBatchXMixedThreadsPerSm = 768;
+// Whether mixed x items run their windows software-pipelined (xpipe_run, at
+// 512 threads per SM: 121 registers).  Items of 4 windows gain too little from
+// it to pay for the lower occupancy: 27.40 G cell-steps/s on the 256-instance
+// batch, against 27.82 G with plain loads at 768 threads per SM.
+constexpr bool kBatchXPipe = false;
 constexpr int kBatchYMixedThreadsPerSm = 448;
 constexpr int kXItemWindows = 4;    // cell windows per x item (one warp's)
 

@@ -95,6 +95,9 @@ __device__ __forceinline__ void batch_sweep_body(const BatchLaunch& L, const Phy
     const typename S::Consts C = S::consts(P);
     const int lane = threadIdx.x & 31;
     const int gwarp = blockIdx.x * (T / 32) + (threadIdx.x >> 5);
+    // The pipelined x items' stage (two windows of two cells per lane, per warp).
+    constexpr bool xpipe = DIR == 1 && S::cells_per_lane == 2 && kBatchXPipe;
+    __shared__ double stage_mem[xpipe ? T / 32 : 1][2][4][xpipe ? 64 : 1];
     int run = -1;
     for (;;) {
         int base = 0;
@@ -113,9 +116,14 @@ __device__ __forceinline__ void batch_sweep_body(const BatchLaunch& L, const Phy
             double cx = 0.0, cy = 0.0;
             if (DIR == 1) {
                 const int rows = min(w.rows, I.ny - w.line);
-                for (int r = 0; r < rows; r++)
-                    for (int j = 0; j < w.wins; j++)
-                        xcell_window<S>(a, C, w.line + r, w.k0 + j, dtdx, cx, cy);
+                if constexpr (xpipe) {
+                    xpipe_run<S>(a, C, stage_mem[threadIdx.x >> 5], w.line, rows, w.k0, w.wins,
+                                 dtdx, cx, cy);
+                } else {
+                    for (int r = 0; r < rows; r++)
+                        for (int j = 0; j < w.wins; j++)
+                            xcell_window<S>(a, C, w.line + r, w.k0 + j, dtdx, cx, cy);
+                }
             } else {
                 const int l = w.line + lane;
                 if (l < a.nlines) {

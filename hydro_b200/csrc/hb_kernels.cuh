@@ -80,6 +80,13 @@ constexpr int kCellThreads = 64;
 constexpr int kFp64MarchMinBlocks = 16;
 constexpr int kFp64CellMinBlocks = 18;
 constexpr int kMixedCellMinBlocks = 12;
+// The software-pipelined mixed x sweep (xpipe_body): two-cell windows per warp
+// and its register cap (8 CTAs of 64 per SM: 119 registers, no spills).  At
+// 4096^2: 0.258 ms with runs of 6 windows, 0.267 with 8, 0.268 with 4, 0.304
+// with 2 (at 12 CTAs per SM and 80 registers, runs of 4: 0.291 ms), against
+// 0.309 ms for one window per warp.
+constexpr int kMixedXPipeWindows = 6;
+constexpr int kMixedXPipeMinBlocks = 8;
 constexpr int kCellWarpOut = 28;   // outputs per warp of the cell-per-lane x sweep
 constexpr int kCellWarpOut2 = 60;  // the same with two cells per lane
 // Outputs per warp of the x sweep window of a stage set.

@@ -412,21 +412,20 @@ __device__ __forceinline__ void xcell_window_1(const SweepArgs& a, const typenam
 // instead of 4 of 32, and each shuffle of primitives, traces or fluxes serves
 // two cells.  Every cell gets the same stage calls on the same inputs as in
 // xcell_window_1.
+// The window's arithmetic on this lane's two cells ka = c - 2 + 2 lane and
+// kb = ka + 1 (ua, ub), already loaded.
 template <class S>
-__device__ __forceinline__ void xcell_window_2(const SweepArgs& a, const typename S::Consts& C,
-                                               int row, int win, double dtdx, double& cx,
-                                               double& cy) {
+__device__ __forceinline__ void xcell_window_2_cells(const SweepArgs& a,
+                                                     const typename S::Consts& C,
+                                                     const LineGeom<1>& g, int c, const Cons& ua,
+                                                     const Cons& ub, double dtdx, double& cx,
+                                                     double& cy) {
     using Prim = typename S::Prim;
     using Flux = typename S::Flux;
     using Sound = typename S::Sound;
     const int lane = threadIdx.x & 31;
-    const int c = win * kCellWarpOut2;               // first output cell of the warp
-    if (c >= a.n - 2) return;                        // warp-uniform
-    const int ka = c - 2 + 2 * lane, kb = ka + 1;    // this lane's two cells
-    const LineGeom<1> g(a, row);
+    const int ka = c - 2 + 2 * lane, kb = ka + 1;
     const typename S::TraceK K = S::trace_constants(C, dtdx);
-    const Cons ua = (ka >= 0 && ka < a.n) ? load_cell<1>(a, g, ka) : Cons{1.0, 0.0, 0.0, 1.0};
-    const Cons ub = (kb >= 0 && kb < a.n) ? load_cell<1>(a, g, kb) : Cons{1.0, 0.0, 0.0, 1.0};
     Prim qa, qb;
     Sound ca, cb;
     S::prim(C, ua, qa, ca);
@@ -465,6 +464,124 @@ __device__ __forceinline__ void xcell_window_2(const SweepArgs& a, const typenam
                 cy = cy > ct ? cy : ct;
             }
         }
+    }
+}
+
+// A cell of the two-cell window: loaded (with the fused boundary fill for
+// ghosts), or a placeholder beyond the line that no output reads.
+__device__ __forceinline__ Cons window_cell(const SweepArgs& a, const LineGeom<1>& g, int k) {
+    return (k >= 0 && k < a.n) ? load_cell<1>(a, g, k) : Cons{1.0, 0.0, 0.0, 1.0};
+}
+
+template <class S>
+__device__ __forceinline__ void xcell_window_2(const SweepArgs& a, const typename S::Consts& C,
+                                               int row, int win, double dtdx, double& cx,
+                                               double& cy) {
+    const int lane = threadIdx.x & 31;
+    const int c = win * kCellWarpOut2;               // first output cell of the warp
+    if (c >= a.n - 2) return;                        // warp-uniform
+    const int ka = c - 2 + 2 * lane;                 // this lane's two cells: ka, ka + 1
+    const LineGeom<1> g(a, row);
+    const Cons ua = window_cell(a, g, ka), ub = window_cell(a, g, ka + 1);
+    xcell_window_2_cells<S>(a, C, g, c, ua, ub, dtdx, cx, cy);
+}
+
+// Software-pipelined runs of two-cell windows: while a window computes, the
+// interior cells of the next one are copied with cp.async into the other half
+// of the warp's shared-memory stage (each lane copies and reads back only its
+// own two cells, so no barrier is needed).
+struct WindowStage {
+    double (*t)[4][64];  // [buffer][variable][cell of the window]
+    __device__ __forceinline__ void issue(const SweepArgs& a, const LineGeom<1>& g, int c,
+                                          int b) const {
+        const int lane = threadIdx.x & 31;
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+            const int k = c - 2 + 2 * lane + e;
+            if (k >= 2 && k < a.n - 2) {
+                const double* p = a.in + g.at(k);
+#pragma unroll
+                for (int v = 0; v < 4; v++) {
+                    const unsigned dst =
+                        (unsigned)__cvta_generic_to_shared(&t[b][v][2 * lane + e]);
+                    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst),
+                                 "l"(p + v * a.vs)
+                                 : "memory");
+                }
+            }
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    }
+    __device__ __forceinline__ void skip() const {
+        asm volatile("cp.async.commit_group;\n" ::: "memory");  // an empty group
+    }
+    // Every group but the most recent one has landed.
+    __device__ __forceinline__ void wait_previous() const {
+        asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+    }
+    __device__ __forceinline__ Cons cell(const SweepArgs& a, const LineGeom<1>& g, int k, int b,
+                                         int e) const {
+        if (k >= 2 && k < a.n - 2) {
+            const int i = 2 * (threadIdx.x & 31) + e;
+            return Cons{t[b][0][i], t[b][Slots<1>::mn][i], t[b][Slots<1>::mt][i], t[b][3][i]};
+        }
+        return window_cell(a, g, k);
+    }
+};
+
+// One warp's windows win0 .. win0 + wins - 1 of rows row0 .. row0 + rows - 1
+// (all valid), in row order, pipelined through the warp's stage.
+template <class S>
+__device__ __forceinline__ void xpipe_run(const SweepArgs& a, const typename S::Consts& C,
+                                          double (*stage)[4][64], int row0, int rows, int win0,
+                                          int wins, double dtdx, double& cx, double& cy) {
+    const WindowStage st{stage};
+    const int lane = threadIdx.x & 31;
+    const int n = rows * wins;
+    st.issue(a, LineGeom<1>(a, row0), win0 * kCellWarpOut2, 0);
+    int r = 0, j = 0;  // window t = r * wins + j
+    for (int t = 0; t < n; t++) {
+        const int b = t & 1;
+        const int r1 = j + 1 < wins ? r : r + 1, j1 = j + 1 < wins ? j + 1 : 0;
+        if (t + 1 < n) st.issue(a, LineGeom<1>(a, row0 + r1), (win0 + j1) * kCellWarpOut2, b ^ 1);
+        else st.skip();
+        st.wait_previous();
+        const LineGeom<1> g(a, row0 + r);
+        const int c = (win0 + j) * kCellWarpOut2;
+        const int ka = c - 2 + 2 * lane;
+        const Cons ua = st.cell(a, g, ka, b, 0), ub = st.cell(a, g, ka + 1, b, 1);
+        xcell_window_2_cells<S>(a, C, g, c, ua, ub, dtdx, cx, cy);
+        r = r1;
+        j = j1;
+    }
+}
+
+// Grid: x = rows, y = ceil(runs of NW windows / warps per CTA).
+template <class S, int NW>
+__device__ __forceinline__ void xpipe_body(const SweepArgs& a, const Phys& P) {
+    __shared__ double stage_mem[kCellThreads / 32][2][4][64];
+    const int warp = threadIdx.x >> 5;
+    const int row = blockIdx.x;
+    const int total = (a.n - 2 + kCellWarpOut2 - 1) / kCellWarpOut2;
+    const int w0 = a.w_lo + (blockIdx.y * (blockDim.x >> 5) + warp) * NW;
+    int w1 = w0 + NW;
+    w1 = w1 < a.w_hi ? w1 : a.w_hi;
+    w1 = w1 < total ? w1 : total;
+    bool active = row < a.nlines && w0 < w1;
+    double dt = a.dt;
+    if (a.clk) {
+        active = active && a.clk->active;
+        dt = a.clk->dt;
+    }
+    double cx = 0.0, cy = 0.0;
+    if (active) {
+        const typename S::Consts C = S::consts(P);
+        xpipe_run<S>(a, C, stage_mem[warp], row, 1, w0, w1 - w0, dt / P.dx, cx, cy);
+    }
+    if (a.courant) {
+        const int slot = cour_slot();
+        warp_max_atomic(&a.courant[slot], cx);
+        warp_max_atomic(&a.courant[kCourSlots + slot], cy);
     }
 }
 

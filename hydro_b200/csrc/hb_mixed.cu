@@ -21,11 +21,27 @@ xcell_mixed_kernel(const SweepArgs a, const Phys P) {
     xcell_body<MixedStages>(a, P);
 }
 
+template <int NW>
+__global__ void __launch_bounds__(kCellThreads, kMixedXPipeMinBlocks)
+xpipe_mixed_kernel(const SweepArgs a, const Phys P) {
+    xpipe_body<MixedStages, NW>(a, P);
+}
+
+// The x sweep: runs of kMixedXPipeWindows pipelined windows per warp when
+// they make at least four waves of the pipelined kernel's resident warps,
+// else one window per warp (small grids need the parallelism more).
 cudaError_t launch_xcell_mixed(const SweepArgs& a, const Phys& P, cudaStream_t s) {
     const int nwin =
         window_span(a, (a.n - 2 + window_out<MixedStages>() - 1) / window_out<MixedStages>());
     const int wpc = kCellThreads / 32;
     if (nwin == 0) return cudaSuccess;
+    constexpr int NW = kMixedXPipeWindows;
+    const long long runs = (long long)a.nlines * ((nwin + NW - 1) / NW);
+    if (runs >= 4LL * device_sm_count() * kMixedXPipeMinBlocks * wpc) {
+        dim3 grid(a.nlines, ((nwin + NW - 1) / NW + wpc - 1) / wpc);
+        xpipe_mixed_kernel<NW><<<grid, kCellThreads, 0, s>>>(a, P);
+        return cudaGetLastError();
+    }
     dim3 grid(a.nlines, (nwin + wpc - 1) / wpc);
     xcell_mixed_kernel<<<grid, kCellThreads, 0, s>>>(a, P);
     return cudaGetLastError();
