@@ -178,14 +178,16 @@ int build_lists(hb_batch* b) {
         const int segs = (I.ny + b->tune.seg - 1) / b->tune.seg;
         add(yl, 1, ItemRun{s, segs, 0, 0}, (long long)groups * segs);
         // x windows of the stage set's width (two cells per lane in mixed precision)
-        const int wout = b->precision == HB_PREC_MIXED ? hb::kCellWarpOut2 : hb::kCellWarpOut;
+        const bool mixed = b->precision == HB_PREC_MIXED;
+        const int wout = mixed ? hb::kCellWarpOut2 : hb::kCellWarpOut;
         const int nwin = (I.nx + 2 + wout - 1) / wout;
-        if (nwin >= hb::kXItemWindows) {
-            const int per = (nwin + hb::kXItemWindows - 1) / hb::kXItemWindows;
+        const int xw = hb::x_item_windows(mixed);
+        if (nwin >= xw) {
+            const int per = (nwin + xw - 1) / xw;
             add(xl, 0, ItemRun{s, per, nwin, 0}, (long long)I.ny * per);
         } else {
             // A narrow grid: whole rows, as many as make up an item's windows.
-            const int rows = hb::kXItemWindows / nwin;
+            const int rows = xw / nwin;
             add(xl, 0, ItemRun{s, -rows, nwin, 0}, (I.ny + rows - 1) / rows);
         }
     }

@@ -54,8 +54,8 @@ struct WorkItem {
 };
 
 // The items of one instance in one list, numbered from `first` in the list:
-//  - x, a grid of at least kXItemWindows windows per row: `per` items per row,
-//    item j covers row j / per, windows from (j % per) * kXItemWindows;
+//  - x, a grid of at least XW = x_item_windows() windows per row: `per` items
+//    per row, item j covers row j / per, windows from (j % per) * XW;
 //  - x, a narrower grid: per = -(rows per item), item j covers rows from
 //    j * rows, all `nwin` windows of each;
 //  - y: `per` row segments per column group, item j is group j / per
@@ -83,7 +83,7 @@ constexpr int kBatchCourSlots = 16; // Courant accumulator slots per instance
 //    latency-bound, and 14 CTAs of 64 are 5% faster per step than 10.
 //  - FP64 y items: 1024, the plain FP64 march's cap (64 registers): 134
 //    registers uncapped, 15% slower per batched step.
-//  - mixed x items: 768 (80 registers), the plain mixed x sweep's.
+//  - mixed x items: 512 (121 registers), pipelined (below).
 //  - mixed y items (marching, cp.async column ring): 448; uncapped they take 147
 //    registers (6 CTAs of 64), 7 CTAs of 64 are 3% faster, 8 less so.
 // The caps need not match the single-grid kernels': no stage set rounds
@@ -92,14 +92,17 @@ constexpr int kBatchCourSlots = 16; // Courant accumulator slots per instance
 // equal their single-grid runs bit for bit under any cap or CTA size.
 constexpr int kBatchXThreadsPerSm = 896;
 constexpr int kBatchYThreadsPerSm = 1024;
-constexpr int kBatchXMixedThreadsPerSm = 768;
-// Whether mixed x items run their windows software-pipelined (xpipe_run, at
-// 512 threads per SM: 121 registers).  Items of 4 windows gain too little from
-// it to pay for the lower occupancy: 27.40 G cell-steps/s on the 256-instance
-// batch, against 27.82 G with plain loads at 768 threads per SM.
-constexpr bool kBatchXPipe = false;
+constexpr int kBatchXMixedThreadsPerSm = 512;
+// Mixed x items run their windows software-pipelined (xpipe_run, at 512
+// threads per SM: 121 registers), in items of up to 12 two-cell windows.  On
+// the 256-instance batch (G cell-steps/s): 28.52 so, 28.33 with items of 8,
+// 27.40 with items of 4; with plain loads at 768 threads per SM, 27.82 (items
+// of 4) and 28.29 (items of 8).
+constexpr bool kBatchXPipe = true;
 constexpr int kBatchYMixedThreadsPerSm = 448;
-constexpr int kXItemWindows = 4;    // cell windows per x item (one warp's)
+// Cell windows per x item (one warp's): FP64 (one cell per lane) 4, mixed
+// (two cells per lane, pipelined) 12.
+__host__ __device__ constexpr int x_item_windows(bool two_cell) { return two_cell ? 12 : 4; }
 
 struct BatchLaunch {
     BatchInst* inst;

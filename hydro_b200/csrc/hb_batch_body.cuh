@@ -54,9 +54,9 @@ __device__ __forceinline__ int find_run(const int* first, int nruns, int it, int
     return lo;
 }
 
-// Item `it` of the list, from its run (ItemRun).  `run` carries the warp's
+// Item `it` of the list, from its run (ItemRun); XW windows per x item.  `run` carries the warp's
 // last run from claim to claim: consecutive claims mostly fall in it.
-template <int DIR>
+template <int DIR, int XW>
 __device__ __forceinline__ WorkItem decode_item(const BatchLaunch& L, int it, int lane, int& run) {
     const bool hit = run >= 0 && __ldg(L.run_first + run) <= it &&
                      (run + 1 == L.nruns || it < __ldg(L.run_first + run + 1));
@@ -72,9 +72,9 @@ __device__ __forceinline__ WorkItem decode_item(const BatchLaunch& L, int it, in
         w.wins = 0;
     } else if (R.per > 0) {
         w.line = j / R.per;
-        w.k0 = (j % R.per) * kXItemWindows;
+        w.k0 = (j % R.per) * XW;
         w.rows = 1;
-        w.wins = min(kXItemWindows, R.nwin - w.k0);
+        w.wins = min(XW, R.nwin - w.k0);
     } else {
         w.line = j * -R.per;
         w.k0 = 0;
@@ -106,7 +106,7 @@ __device__ __forceinline__ void batch_sweep_body(const BatchLaunch& L, const Phy
         if (base >= L.nitems) break;
         const int end = min(base + L.claim, L.nitems);
         for (int it = base; it < end; it++) {
-            const WorkItem w = decode_item<DIR>(L, it, lane, run);
+            const WorkItem w = decode_item<DIR, x_item_windows(S::cells_per_lane == 2)>(L, it, lane, run);
             BatchInst* Ip = L.inst + w.slot;
             const BatchInst I = *Ip;
             if (!I.active) continue;  // warp-uniform
