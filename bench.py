@@ -326,6 +326,49 @@ def run_energy_noise_form(H, K, W, pg, device, world, seed=20261205):
     return out
 
 
+def run_mixed_bulk_x(H, u0, K, W, pg, device, world, want):
+    """The mixed form with its x sweep staged by TMA-engine bulk copies
+    (kernel "bulk") over the same steps: whole-job rate, the mean x-sweep
+    launch time beside the default x kernel's, and bitwise equality of the
+    final state with the default kernels' (`want`)."""
+    import torch
+    from hydro_b200 import Domain
+    out = {}
+    for k in ("bulk", "auto"):
+        d = Domain(H, precision="mixed", kernels=(k, None))
+        d.upload(u0)
+        d.set_clock()
+        d.launch_steps(W)
+        d.synchronize()
+        d.upload(u0)
+        d.set_clock()
+        st = torch.cuda.ExternalStream(d.stream_ptr, device=device)
+        barrier(pg, device)
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record(st)
+        d.launch_steps(K)
+        g1.record(st)
+        g1.synchronize()
+        d.synchronize()
+        ms = all_max(pg, g0.elapsed_time(g1), device)
+        if k == "bulk":
+            got = d.download()
+            out["value"] = round(world * H.nx * H.ny * K / (ms / 1e3) / 1e6, 3)
+            out["unit"] = "Mcell-updates/s"
+            out["bitwise_equal_to_default"] = bool(np.array_equal(got.view(np.uint64),
+                                                                  want.view(np.uint64)))
+            del got
+        d.upload(u0)
+        d.set_clock()
+        d.profile(True)
+        d.profile_read(reset=True)
+        d.launch_steps(K)
+        msx, _, nx_, _ = d.profile_read(reset=True)
+        out["x_sweep_ms" if k == "bulk" else "default_x_sweep_ms"] = round(msx / max(nx_, 1), 4)
+        d.close()
+    return out
+
+
 def run_noalloc_form(device):
     """The allocation-free step against the regular domain step on the same
     grids (CUDA events, fixed dt, 50 steps each after 5 warm-up steps)."""
@@ -830,12 +873,16 @@ def main():
         g1.synchronize()
         mix_ms = all_max(pg, g0.elapsed_time(g1), device)
         mix_state = dm.download()
+        mix_kernels = dm.kernels()
         dm.close()
+        bulk = run_mixed_bulk_x(H, u0, K, W, pg, device, world, mix_state)
         err = field_errors(mix_state, ref_state)
         forms["mixed"] = {"value": round(world * nx * ny * K / (mix_ms / 1e3) / 1e6, 3),
                           "unit": "Mcell-updates/s", "ms_per_step": round(mix_ms / K, 4),
                           "speedup_vs_fp64": round(ms_max / mix_ms, 3),
                           "errors_vs_fp64": err,
+                          "kernels": {"x": mix_kernels[0], "y": mix_kernels[1]},
+                          "x_bulk_copy_staging": bulk,
                           "precision": "FP32 stages; FP64 Newton p*, update, Courant"}
         if rank == 0 and world == 1:
             forms["mixed"]["beside_reference_fp32_build"] = mixed_beside_reference_fp32()

@@ -24,8 +24,9 @@ HB_XSWEEP_MARCH, HB_XSWEEP_CELL = 0, 1
 HB_NOALLOC_MAX_CELLS = 1 << 20  # include/hydro_b200.h
 XSWEEPS = {"march": HB_XSWEEP_MARCH, "cell": HB_XSWEEP_CELL}
 HB_KERNEL_AUTO, HB_KERNEL_MARCH, HB_KERNEL_WARP, HB_KERNEL_COOP, HB_KERNEL_COOP8 = -1, 0, 1, 2, 3
+HB_KERNEL_BULK = 4
 KERNELS = {"auto": HB_KERNEL_AUTO, "march": HB_KERNEL_MARCH, "warp": HB_KERNEL_WARP,
-           "coop": HB_KERNEL_COOP, "coop8": HB_KERNEL_COOP8}
+           "coop": HB_KERNEL_COOP, "coop8": HB_KERNEL_COOP8, "bulk": HB_KERNEL_BULK}
 
 
 class HydroParam(C.Structure):

@@ -97,7 +97,7 @@ __device__ __forceinline__ void batch_sweep_body(const BatchLaunch& L, const Phy
     const int gwarp = blockIdx.x * (T / 32) + (threadIdx.x >> 5);
     // The pipelined x items' stage (two windows of two cells per lane, per warp).
     constexpr bool xpipe = DIR == 1 && S::cells_per_lane == 2 && kBatchXPipe;
-    __shared__ double stage_mem[xpipe ? T / 32 : 1][2][4][xpipe ? 64 : 1];
+    __shared__ WindowStageMem stage_mem[xpipe ? T / 32 : 1];
     int run = -1;
     for (;;) {
         int base = 0;
@@ -117,8 +117,8 @@ __device__ __forceinline__ void batch_sweep_body(const BatchLaunch& L, const Phy
             if (DIR == 1) {
                 const int rows = min(w.rows, I.ny - w.line);
                 if constexpr (xpipe) {
-                    xpipe_run<S>(a, C, stage_mem[threadIdx.x >> 5], w.line, rows, w.k0, w.wins,
-                                 dtdx, cx, cy);
+                    xpipe_run<S, WindowStage>(a, C, &stage_mem[threadIdx.x >> 5], w.line, rows,
+                                              w.k0, w.wins, dtdx, cx, cy);
                 } else {
                     for (int r = 0; r < rows; r++)
                         for (int j = 0; j < w.wins; j++)

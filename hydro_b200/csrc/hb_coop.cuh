@@ -52,10 +52,13 @@ __device__ __forceinline__ typename S::Prim coop_get(const typename S::Real (*sr
 // `active` false makes a thread take part in the barriers only.  Warps whose
 // cells all lie past the line's end skip the arithmetic.  Accumulates the
 // fused Courant maxima of its outputs into cx, cy.
+// `staged`: the window's interior cells are already in the stage (thread t's
+// cell in staged[v][t], coop_stage_issue), else they are loaded here.
 template <class S, int DIR, int G>
 __device__ __forceinline__ void coop_window(const SweepArgs& a, const typename S::Consts& C,
                                             int line, int win, double dtdx, bool active,
-                                            double& cx, double& cy, CoopSmem<S, G>& sm) {
+                                            double& cx, double& cy, CoopSmem<S, G>& sm,
+                                            const double (*staged)[32 * G] = nullptr) {
     using Prim = typename S::Prim;
     using Flux = typename S::Flux;
     constexpr int T = 32 * G, N = T - 4;
@@ -73,7 +76,11 @@ __device__ __forceinline__ void coop_window(const SweepArgs& a, const typename S
     Prim q = S::zero_prim();
     typename S::Sound cs = S::zero_sound();
     if (work) {
-        if (k >= 0 && k < a.n) u = load_cell<DIR>(a, g, k);
+        constexpr int mn = Slots<DIR>::mn, mt = Slots<DIR>::mt;
+        if (staged && k >= 2 && k < a.n - 2)
+            u = Cons{staged[0][t], staged[mn][t], staged[mt][t], staged[3][t]};
+        else if (k >= 0 && k < a.n)
+            u = load_cell<DIR>(a, g, k);
         S::prim(C, u, q, cs);
         coop_put<S, G>(sm.q, t, q);
     }
@@ -132,6 +139,68 @@ __device__ __forceinline__ void coop_body(const SweepArgs& a, const Phys& P) {
     double cx = 0.0, cy = 0.0;
     const typename S::Consts C = S::consts(P);
     coop_window<S, DIR, G>(a, C, line, win, dt / P.dx, active, cx, cy, sm);
+    if (a.courant) {
+        const int slot = cour_slot();
+        warp_max_atomic(&a.courant[slot], cx);
+        warp_max_atomic(&a.courant[kCourSlots + slot], cy);
+    }
+}
+
+// Copies thread t's interior cell of window `win` into stage[v][t] with
+// cp.async (one commit group; empty for a ghost or out-of-line cell).
+template <int DIR, int G>
+__device__ __forceinline__ void coop_stage_issue(const SweepArgs& a, const LineGeom<DIR>& g,
+                                                 int win, double (*stage)[32 * G]) {
+    constexpr int N = 32 * G - 4;
+    const int t = threadIdx.x;
+    const int k = win * N - 2 + t;
+    if (k >= 2 && k < a.n - 2) {
+        const double* p = a.in + g.at(k);
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+            const unsigned dst = (unsigned)__cvta_generic_to_shared(&stage[v][t]);
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst),
+                         "l"(p + v * a.vs)
+                         : "memory");
+        }
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+
+// Grid: x = lines, y = runs of NW consecutive windows.  A CTA sweeps its run
+// software-pipelined: while a window computes, each thread copies its cell of
+// the next window into the other half of a shared-memory stage (its own slot
+// only, so the copies need no barrier of their own).
+template <class S, int DIR, int G, int NW>
+__device__ __forceinline__ void coop_pipe_body(const SweepArgs& a, const Phys& P) {
+    __shared__ CoopSmem<S, G> sm;
+    __shared__ double stage[2][4][32 * G];
+    const int line = blockIdx.x;
+    const int total = (a.n - 2 + (32 * G - 4) - 1) / (32 * G - 4);
+    const int w0 = a.w_lo + (int)blockIdx.y * NW;
+    int w1 = w0 + NW;
+    w1 = w1 < a.w_hi ? w1 : a.w_hi;
+    w1 = w1 < total ? w1 : total;
+    bool active = line < a.nlines && w0 < w1;   // uniform over the CTA
+    double dt = a.dt;
+    if (a.clk) {
+        active = active && a.clk->active;
+        dt = a.clk->dt;
+    }
+    double cx = 0.0, cy = 0.0;
+    if (active) {
+        const typename S::Consts C = S::consts(P);
+        const LineGeom<DIR> g(a, line);
+        coop_stage_issue<DIR, G>(a, g, w0, stage[0]);
+        for (int w = w0; w < w1; w++) {
+            const int b = (w - w0) & 1;
+            if (w + 1 < w1) coop_stage_issue<DIR, G>(a, g, w + 1, stage[b ^ 1]);
+            else asm volatile("cp.async.commit_group;\n" ::: "memory");
+            asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+            coop_window<S, DIR, G>(a, C, line, w, dt / P.dx, true, cx, cy, sm, stage[b]);
+            __syncthreads();  // the window's shared memory is free for the next one
+        }
+    }
     if (a.courant) {
         const int slot = cour_slot();
         warp_max_atomic(&a.courant[slot], cx);

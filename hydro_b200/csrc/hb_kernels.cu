@@ -87,10 +87,27 @@ coop_kernel(const SweepArgs a, const Phys P) {
     coop_body<ExactStages<UNIT>, DIR, G>(a, P);
 }
 
+// The cooperative window over runs of NW windows per CTA, software-pipelined
+// (coop_pipe_body).
+template <bool UNIT, int DIR, int G, int NW>
+__global__ void __launch_bounds__(32 * G, kFp64CoopPipeMinBlocks)
+coop_pipe_kernel(const SweepArgs a, const Phys P) {
+    coop_pipe_body<ExactStages<UNIT>, DIR, G, NW>(a, P);
+}
+
 template <int G>
 static cudaError_t launch_coop_g(int dir, const SweepArgs& a, const Phys& P, cudaStream_t s) {
     const int nwin = window_span(a, coop_windows<G>(a.n));
     if (nwin == 0) return cudaSuccess;
+    if constexpr (kFp64CoopPipeWindows > 1 && G == 4) {
+        constexpr int NW = kFp64CoopPipeWindows > 1 ? kFp64CoopPipeWindows : 2;
+        if (dir == 1) {
+            const dim3 pgrid(a.nlines, (nwin + NW - 1) / NW);
+            if (P.unit_slope) coop_pipe_kernel<true, 1, G, NW><<<pgrid, 32 * G, 0, s>>>(a, P);
+            else coop_pipe_kernel<false, 1, G, NW><<<pgrid, 32 * G, 0, s>>>(a, P);
+            return cudaGetLastError();
+        }
+    }
     const dim3 grid(a.nlines, nwin);
     if (dir == 1) {
         if (P.unit_slope) coop_kernel<true, 1, G><<<grid, 32 * G, 0, s>>>(a, P);

@@ -87,6 +87,11 @@ constexpr int kMixedCellMinBlocks = 12;
 // 0.309 ms for one window per warp.
 constexpr int kMixedXPipeWindows = 6;
 constexpr int kMixedXPipeMinBlocks = 8;
+// The FP64 cooperative x window over software-pipelined runs of windows per
+// CTA (coop_pipe_body; 0 or 1: one window per CTA) and its minimum CTAs of
+// 128 threads per SM.
+constexpr int kFp64CoopPipeWindows = 0;
+constexpr int kFp64CoopPipeMinBlocks = 9;
 constexpr int kCellWarpOut = 28;   // outputs per warp of the cell-per-lane x sweep
 constexpr int kCellWarpOut2 = 60;  // the same with two cells per lane
 // Outputs per warp of the x sweep window of a stage set.
@@ -98,7 +103,12 @@ cudaError_t launch_coop(int dir, int warps, const SweepArgs& a, const Phys& P, c
 cudaError_t launch_coop_mixed(int dir, int warps, const SweepArgs& a, const Phys& P,
                               cudaStream_t s);
 cudaError_t launch_ycell(const SweepArgs& a, const Phys& P, cudaStream_t s);
-cudaError_t launch_xcell_mixed(const SweepArgs& a, const Phys& P, cudaStream_t s);
+// The mixed x sweep (two-cell windows); `bulk`: staged by TMA-engine bulk
+// copies (HB_KERNEL_BULK) instead of per-lane cp.async.
+cudaError_t launch_xcell_mixed(const SweepArgs& a, const Phys& P, cudaStream_t s,
+                               bool bulk = false);
+// Waits of the mixed x sweep's bulk-copy stage that gave up (hb_mixed.cu).
+int mixed_stage_wait_timeouts(bool reset);
 // The FMA FP64 stage set (hb_fast.cu): kernel = HB_KERNEL_* (include/hydro_b200.h).
 cudaError_t launch_sweep_fast(int dir, int kernel, const SweepArgs& a, const Phys& P,
                               cudaStream_t s);

@@ -487,11 +487,25 @@ __device__ __forceinline__ void xcell_window_2(const SweepArgs& a, const typenam
 }
 
 // Software-pipelined runs of two-cell windows: while a window computes, the
-// interior cells of the next one are copied with cp.async into the other half
-// of the warp's shared-memory stage (each lane copies and reads back only its
-// own two cells, so no barrier is needed).
+// interior cells of the next one are copied into the other half of the warp's
+// shared-memory stage.  Two ways to copy:
+//  - WindowStage: each lane copies its own two cells with cp.async and reads
+//    back only those, so no barrier is needed;
+//  - BulkWindowStage: lane 0 copies each variable's interior span with one
+//    bulk copy of the TMA engine (cp.async.bulk), completing on the buffer's
+//    mbarrier, on which the warp waits.
+// A stage row holds 66 cells: a bulk copy starts at the 16-byte boundary at or
+// below the window's first interior cell, so the row may start one cell early.
+constexpr int kStageRow = 66;
+struct alignas(16) WindowStageMem {
+    double t[2][4][kStageRow];   // [buffer][variable][cell of the window (+ shift)]
+    unsigned long long bar[2];   // the bulk copies' mbarriers, one per buffer
+};
+
 struct WindowStage {
-    double (*t)[4][64];  // [buffer][variable][cell of the window]
+    WindowStageMem* m;
+    __device__ __forceinline__ void begin() const {}
+    __device__ __forceinline__ void end() const {}
     __device__ __forceinline__ void issue(const SweepArgs& a, const LineGeom<1>& g, int c,
                                           int b) const {
         const int lane = threadIdx.x & 31;
@@ -503,7 +517,7 @@ struct WindowStage {
 #pragma unroll
                 for (int v = 0; v < 4; v++) {
                     const unsigned dst =
-                        (unsigned)__cvta_generic_to_shared(&t[b][v][2 * lane + e]);
+                        (unsigned)__cvta_generic_to_shared(&m->t[b][v][2 * lane + e]);
                     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst),
                                  "l"(p + v * a.vs)
                                  : "memory");
@@ -515,15 +529,107 @@ struct WindowStage {
     __device__ __forceinline__ void skip() const {
         asm volatile("cp.async.commit_group;\n" ::: "memory");  // an empty group
     }
-    // Every group but the most recent one has landed.
-    __device__ __forceinline__ void wait_previous() const {
+    // Window t's copies have landed: every group but the most recent one.
+    __device__ __forceinline__ void wait(int) const {
         asm volatile("cp.async.wait_group 1;\n" ::: "memory");
     }
-    __device__ __forceinline__ Cons cell(const SweepArgs& a, const LineGeom<1>& g, int k, int b,
-                                         int e) const {
+    __device__ __forceinline__ Cons cell(const SweepArgs& a, const LineGeom<1>& g, int c, int k,
+                                         int b) const {
         if (k >= 2 && k < a.n - 2) {
-            const int i = 2 * (threadIdx.x & 31) + e;
-            return Cons{t[b][0][i], t[b][Slots<1>::mn][i], t[b][Slots<1>::mt][i], t[b][3][i]};
+            const int i = k - (c - 2);
+            return Cons{m->t[b][0][i], m->t[b][Slots<1>::mn][i], m->t[b][Slots<1>::mt][i],
+                        m->t[b][3][i]};
+        }
+        return window_cell(a, g, k);
+    }
+};
+
+// Waits on a bulk copy's mbarrier that gave up (a copy that never completed);
+// the host reads and clears the count (hydro_b200_domain_synchronize).
+static __device__ unsigned int g_stage_wait_timeouts;
+constexpr int kStageWaitSpins = 1 << 20;  // bounded: each try_wait suspends briefly
+
+struct BulkWindowStage {
+    WindowStageMem* m;
+    __device__ __forceinline__ unsigned bar(int b) const {
+        return (unsigned)__cvta_generic_to_shared(&m->bar[b]);
+    }
+    // Before the run's first copy / after its last wait: the warp's barriers
+    // (4 arrivals a phase, one per variable's copy) are set up and torn down
+    // by lane 0, with no copy in flight.
+    __device__ __forceinline__ void begin() const {
+        __syncwarp();
+        if ((threadIdx.x & 31) == 0) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 4;\n" ::"r"(bar(0)) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 4;\n" ::"r"(bar(1)) : "memory");
+            asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        }
+        __syncwarp();
+    }
+    __device__ __forceinline__ void end() const {
+        __syncwarp();
+        if ((threadIdx.x & 31) == 0) {
+            asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(bar(0)) : "memory");
+            asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(bar(1)) : "memory");
+        }
+        __syncwarp();
+    }
+    // Cell shift of variable v's stage row: 1 when the variable's row starts
+    // on an odd 8-byte slot (the copy then starts one cell early).
+    __device__ __forceinline__ static int shift(const SweepArgs& a, const LineGeom<1>& g, int v) {
+        return (int)((reinterpret_cast<uintptr_t>(a.in + g.at(0) + v * a.vs) >> 3) & 1);
+    }
+    // The window at c: cells kA = max(c - 2, 2) .. kB = min(c + 61, n - 3) of
+    // each variable, from the 16-byte boundary at or below cell kA (one cell
+    // early when shift() is 1; kA is even), rounded up to whole 16 bytes (at
+    // most cell kB + 1 <= n - 2, in the row).  Row position kA - (c - 2) is
+    // even, so the destination is 16-byte aligned.  Lane v copies variable v.
+    __device__ __forceinline__ void issue(const SweepArgs& a, const LineGeom<1>& g, int c,
+                                          int b) const {
+        __syncwarp();  // every lane has read the buffer's previous window
+        const int v = threadIdx.x & 31;
+        if (v < 4) {
+            const int kA = c - 2 > 2 ? c - 2 : 2;
+            const int kB = c + 61 < a.n - 3 ? c + 61 : a.n - 3;
+            const int d = shift(a, g, v);
+            const double* src = a.in + g.at(kA) + v * a.vs - d;
+            const unsigned bytes = ((unsigned)(kB - kA + 1 + d) * 8u + 15u) & ~15u;
+            const unsigned dst = (unsigned)__cvta_generic_to_shared(&m->t[b][v][kA - (c - 2)]);
+            asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar(b)),
+                         "r"(bytes)
+                         : "memory");
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes "
+                "[%0], [%1], %2, [%3];\n" ::"r"(dst),
+                "l"(src), "r"(bytes), "r"(bar(b))
+                : "memory");
+        }
+    }
+    __device__ __forceinline__ void skip() const {}
+    // Window t's copies have landed: buffer t & 1 completes its (t >> 1)-th phase.
+    __device__ __forceinline__ void wait(int t) const {
+        const unsigned addr = bar(t & 1), parity = (unsigned)(t >> 1) & 1u;
+        unsigned ok = 0;
+        for (int i = 0; i < kStageWaitSpins && !ok; i++)
+            asm volatile(
+                "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                " selp.u32 %0, 1, 0, p;\n}\n"
+                : "=r"(ok)
+                : "r"(addr), "r"(parity)
+                : "memory");
+        if (!ok) atomicAdd(&g_stage_wait_timeouts, 1u);
+    }
+    __device__ __forceinline__ Cons cell(const SweepArgs& a, const LineGeom<1>& g, int c, int k,
+                                         int b) const {
+        if (k >= 2 && k < a.n - 2) {
+            const int i = k - (c - 2);
+            // Shifts of the four rows: the row start's parity, plus v times the
+            // variable stride's.
+            const int s0 = shift(a, g, 0), sv = (int)(a.vs & 1);
+            return Cons{m->t[b][0][i + s0], m->t[b][Slots<1>::mn][i + ((s0 + sv) & 1)],
+                        m->t[b][Slots<1>::mt][i + ((s0 + 2 * sv) & 1)],
+                        m->t[b][3][i + ((s0 + 3 * sv) & 1)]};
         }
         return window_cell(a, g, k);
     }
@@ -531,13 +637,14 @@ struct WindowStage {
 
 // One warp's windows win0 .. win0 + wins - 1 of rows row0 .. row0 + rows - 1
 // (all valid), in row order, pipelined through the warp's stage.
-template <class S>
+template <class S, class Stage>
 __device__ __forceinline__ void xpipe_run(const SweepArgs& a, const typename S::Consts& C,
-                                          double (*stage)[4][64], int row0, int rows, int win0,
+                                          WindowStageMem* mem, int row0, int rows, int win0,
                                           int wins, double dtdx, double& cx, double& cy) {
-    const WindowStage st{stage};
+    const Stage st{mem};
     const int lane = threadIdx.x & 31;
     const int n = rows * wins;
+    st.begin();
     st.issue(a, LineGeom<1>(a, row0), win0 * kCellWarpOut2, 0);
     int r = 0, j = 0;  // window t = r * wins + j
     for (int t = 0; t < n; t++) {
@@ -545,21 +652,22 @@ __device__ __forceinline__ void xpipe_run(const SweepArgs& a, const typename S::
         const int r1 = j + 1 < wins ? r : r + 1, j1 = j + 1 < wins ? j + 1 : 0;
         if (t + 1 < n) st.issue(a, LineGeom<1>(a, row0 + r1), (win0 + j1) * kCellWarpOut2, b ^ 1);
         else st.skip();
-        st.wait_previous();
+        st.wait(t);
         const LineGeom<1> g(a, row0 + r);
         const int c = (win0 + j) * kCellWarpOut2;
         const int ka = c - 2 + 2 * lane;
-        const Cons ua = st.cell(a, g, ka, b, 0), ub = st.cell(a, g, ka + 1, b, 1);
+        const Cons ua = st.cell(a, g, c, ka, b), ub = st.cell(a, g, c, ka + 1, b);
         xcell_window_2_cells<S>(a, C, g, c, ua, ub, dtdx, cx, cy);
         r = r1;
         j = j1;
     }
+    st.end();
 }
 
 // Grid: x = rows, y = ceil(runs of NW windows / warps per CTA).
-template <class S, int NW>
+template <class S, int NW, class Stage>
 __device__ __forceinline__ void xpipe_body(const SweepArgs& a, const Phys& P) {
-    __shared__ double stage_mem[kCellThreads / 32][2][4][64];
+    __shared__ WindowStageMem stage_mem[kCellThreads / 32];
     const int warp = threadIdx.x >> 5;
     const int row = blockIdx.x;
     const int total = (a.n - 2 + kCellWarpOut2 - 1) / kCellWarpOut2;
@@ -576,7 +684,7 @@ __device__ __forceinline__ void xpipe_body(const SweepArgs& a, const Phys& P) {
     double cx = 0.0, cy = 0.0;
     if (active) {
         const typename S::Consts C = S::consts(P);
-        xpipe_run<S>(a, C, stage_mem[warp], row, 1, w0, w1 - w0, dt / P.dx, cx, cy);
+        xpipe_run<S, Stage>(a, C, &stage_mem[warp], row, 1, w0, w1 - w0, dt / P.dx, cx, cy);
     }
     if (a.courant) {
         const int slot = cour_slot();

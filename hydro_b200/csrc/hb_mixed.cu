@@ -21,25 +21,43 @@ xcell_mixed_kernel(const SweepArgs a, const Phys P) {
     xcell_body<MixedStages>(a, P);
 }
 
-template <int NW>
+template <int NW, class Stage>
 __global__ void __launch_bounds__(kCellThreads, kMixedXPipeMinBlocks)
 xpipe_mixed_kernel(const SweepArgs a, const Phys P) {
-    xpipe_body<MixedStages, NW>(a, P);
+    xpipe_body<MixedStages, NW, Stage>(a, P);
+}
+
+// Waits on the bulk-copy stage's mbarriers that gave up since the last call
+// (g_stage_wait_timeouts of this translation unit), cleared when `reset`;
+// -1 if the count cannot be read.
+int mixed_stage_wait_timeouts(bool reset) {
+    unsigned v = 0;
+    if (cudaMemcpyFromSymbol(&v, g_stage_wait_timeouts, sizeof v) != cudaSuccess) return -1;
+    if (v && reset) {
+        const unsigned z = 0;
+        if (cudaMemcpyToSymbol(g_stage_wait_timeouts, &z, sizeof z) != cudaSuccess) return -1;
+    }
+    return (int)v;
 }
 
 // The x sweep: runs of kMixedXPipeWindows pipelined windows per warp when
 // they make at least four waves of the pipelined kernel's resident warps,
-// else one window per warp (small grids need the parallelism more).
-cudaError_t launch_xcell_mixed(const SweepArgs& a, const Phys& P, cudaStream_t s) {
+// else one window per warp (small grids need the parallelism more).  `bulk`
+// always takes the pipelined runs, staged by bulk copies.
+cudaError_t launch_xcell_mixed(const SweepArgs& a, const Phys& P, cudaStream_t s, bool bulk) {
     const int nwin =
         window_span(a, (a.n - 2 + window_out<MixedStages>() - 1) / window_out<MixedStages>());
     const int wpc = kCellThreads / 32;
     if (nwin == 0) return cudaSuccess;
     constexpr int NW = kMixedXPipeWindows;
     const long long runs = (long long)a.nlines * ((nwin + NW - 1) / NW);
+    const dim3 pgrid(a.nlines, ((nwin + NW - 1) / NW + wpc - 1) / wpc);
+    if (bulk) {
+        xpipe_mixed_kernel<NW, BulkWindowStage><<<pgrid, kCellThreads, 0, s>>>(a, P);
+        return cudaGetLastError();
+    }
     if (runs >= 4LL * device_sm_count() * kMixedXPipeMinBlocks * wpc) {
-        dim3 grid(a.nlines, ((nwin + NW - 1) / NW + wpc - 1) / wpc);
-        xpipe_mixed_kernel<NW><<<grid, kCellThreads, 0, s>>>(a, P);
+        xpipe_mixed_kernel<NW, WindowStage><<<pgrid, kCellThreads, 0, s>>>(a, P);
         return cudaGetLastError();
     }
     dim3 grid(a.nlines, (nwin + wpc - 1) / wpc);

@@ -293,6 +293,9 @@ extern "C" int hydro_b200_domain_download(hb_domain* d, double* host) {
 extern "C" int hydro_b200_domain_synchronize(hb_domain* d) {
     if (!d) return set_error(HB_ERR_ARG, "null domain");
     HB_CU(cudaStreamSynchronize(d->stream));
+    if (d->precision == HB_PREC_MIXED && d->kern[HB_PREC_MIXED][1] == HB_KERNEL_BULK &&
+        hb::mixed_stage_wait_timeouts(true) != 0)
+        return set_error(HB_ERR_CUDA, "a staged bulk copy of the mixed x sweep did not complete");
     return HB_OK;
 }
 
@@ -353,8 +356,8 @@ static int launch_sweep_timed(hb_domain* d, int dir, const SweepArgs& a) {
     } else if (d->precision == HB_PREC_MIXED) {
         if (kern == HB_KERNEL_COOP || kern == HB_KERNEL_COOP8)
             HB_CU(hb::launch_coop_mixed(dir, kern == HB_KERNEL_COOP8 ? 8 : 4, a, d->P, d->stream));
-        else if (kern == HB_KERNEL_WARP && dir == 1)
-            HB_CU(hb::launch_xcell_mixed(a, d->P, d->stream));
+        else if ((kern == HB_KERNEL_WARP || kern == HB_KERNEL_BULK) && dir == 1)
+            HB_CU(hb::launch_xcell_mixed(a, d->P, d->stream, kern == HB_KERNEL_BULK));
         else
             HB_CU(hb::launch_sweep_mixed(dir, a, d->P, d->stream));
     } else {
@@ -438,7 +441,8 @@ static void window_bounds(const hb_domain* d, int dir, int* total, int* lo, int*
         int W = hb::kCellWarpOut;
         if (kern == HB_KERNEL_COOP) W = 32 * 4 - 4;
         if (kern == HB_KERNEL_COOP8) W = 32 * 8 - 4;
-        if (kern == HB_KERNEL_WARP && dir == 1 && d->precision == HB_PREC_MIXED)
+        if ((kern == HB_KERNEL_WARP || kern == HB_KERNEL_BULK) && dir == 1 &&
+            d->precision == HB_PREC_MIXED)
             W = hb::kCellWarpOut2;
         *total = (n - 2 + W - 1) / W;
         *lo = 1;
@@ -561,9 +565,12 @@ extern "C" int hydro_b200_domain_set_kernel(hb_domain* d, int precision, int idi
         return set_error(HB_ERR_ARG, "precision=%d idim=%d: invalid", precision, idim);
     if (kernel == HB_KERNEL_AUTO) kernel = default_kernel(d, precision, idim);
     const bool known = kernel == HB_KERNEL_MARCH || kernel == HB_KERNEL_WARP ||
-                       kernel == HB_KERNEL_COOP || kernel == HB_KERNEL_COOP8;
-    // The mixed set has no warp window along columns.
-    if (!known || (precision == HB_PREC_MIXED && idim == 2 && kernel == HB_KERNEL_WARP))
+                       kernel == HB_KERNEL_COOP || kernel == HB_KERNEL_COOP8 ||
+                       kernel == HB_KERNEL_BULK;
+    // The mixed set has no warp window along columns; bulk staging exists for
+    // the mixed x sweep only.
+    if (!known || (precision == HB_PREC_MIXED && idim == 2 && kernel == HB_KERNEL_WARP) ||
+        (kernel == HB_KERNEL_BULK && (precision != HB_PREC_MIXED || idim != 1)))
         return set_error(HB_ERR_ARG, "kernel=%d: not available for precision %d, idim %d", kernel,
                          precision, idim);
     d->kern[precision][idim] = kernel;

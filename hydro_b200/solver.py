@@ -140,7 +140,8 @@ class Domain:
 
     def set_kernels(self, x: str | None = None, y: str | None = None) -> None:
         """Sweep kernels of this domain's precision: "march", "warp", "coop",
-        "coop8" or "auto" per direction (None keeps the current one)."""
+        "coop8", "bulk" (mixed x sweep only) or "auto" per direction (None
+        keeps the current one)."""
         prec = _lib.PRECISIONS[self.precision]
         for idim, k in ((1, x), (2, y)):
             if k is not None:

@@ -272,6 +272,12 @@ int hydro_b200_domain_set_xsweep(hb_domain *d, int precision, int mode);
  *   HB_KERNEL_COOP   a CTA of 4 warps takes 128 consecutive cells of a line,
  *                    neighbours through shared memory: 124 outputs per CTA;
  *   HB_KERNEL_COOP8  the same with 8 warps: 252 outputs per CTA;
+ *   HB_KERNEL_BULK   mixed x sweep only: runs of two-cell warp windows whose
+ *                    cells are staged in shared memory by bulk copies of the
+ *                    TMA engine (cp.async.bulk, mbarrier completion) while the
+ *                    previous window computes; results identical to
+ *                    HB_KERNEL_WARP, whose large-grid form stages by per-lane
+ *                    cp.async;
  *   HB_KERNEL_AUTO   the measured default for the grid size.
  * get_kernel returns the current choice (-1 on error). */
 #define HB_KERNEL_AUTO (-1)
@@ -279,6 +285,7 @@ int hydro_b200_domain_set_xsweep(hb_domain *d, int precision, int mode);
 #define HB_KERNEL_WARP 1
 #define HB_KERNEL_COOP 2
 #define HB_KERNEL_COOP8 3
+#define HB_KERNEL_BULK 4
 int hydro_b200_domain_set_kernel(hb_domain *d, int precision, int idim, int kernel);
 int hydro_b200_domain_get_kernel(hb_domain *d, int precision, int idim);
 

@@ -175,3 +175,34 @@ def test_mixed_contact_with_equal_pressure_and_velocity(product_lib, vel):
         assert np.allclose(m[1] / m[0], vel, rtol=0, atol=1e-5)
         pm = (H.gamma - 1.0) * (m[3] - 0.5 * m[1] ** 2 / m[0])
         assert np.allclose(pm, p, rtol=1e-5, atol=0)
+
+
+@pytest.mark.parametrize("nx,ny", [(2047, 2050), (3001, 777), (250, 125), (64, 40)])
+def test_mixed_bulk_copy_staging_is_bitwise_the_default(product_lib, nx, ny):
+    """The mixed x sweep staged by bulk copies of the TMA engine (kernel
+    "bulk": mbarrier completion, rows starting on either 16-byte alignment)
+    gives the same bits as the default x kernel (per-lane cp.async staging on
+    large grids, plain loads on small ones)."""
+    from _helpers import bitwise_equal
+    H = make_params(nx, ny, testcase=1)
+    u0 = init_noisy_blast(H, 9, testcase=1, var=3)
+    out = []
+    for k in ("auto", "bulk"):
+        d = Domain(H, precision="mixed", kernels=(k, None))
+        d.upload(u0)
+        d.set_clock()
+        d.launch_steps(12)
+        d.synchronize()   # raises if a staged copy's wait gave up
+        out.append(d.download())
+        assert d.kernels()[0] == ("bulk" if k == "bulk" else "warp")
+        d.close()
+    assert bitwise_equal(out[0], out[1])
+
+
+def test_bulk_kernel_only_for_the_mixed_x_sweep(product_lib):
+    from hydro_b200._lib import HydroB200Error
+    H = make_params(64, 40, testcase=1)
+    with pytest.raises(HydroB200Error):
+        Domain(H, precision="fp64", kernels=("bulk", None))
+    with pytest.raises(HydroB200Error):
+        Domain(H, precision="mixed", kernels=(None, "bulk"))
