@@ -882,6 +882,12 @@ def main():
                           "speedup_vs_fp64": round(ms_max / mix_ms, 3),
                           "errors_vs_fp64": err,
                           "kernels": {"x": mix_kernels[0], "y": mix_kernels[1]},
+                          # the same 128 B per cell-step of FP64 state as the plain path
+                          "hbm_gbs_per_step": round(world * nx * ny * K * BYTES_PER_CELL_STEP
+                                                    / (mix_ms / 1e3) / 1e9, 1),
+                          "hbm_frac_of_measured_peak": round(
+                              world * nx * ny * K * BYTES_PER_CELL_STEP / (mix_ms / 1e3) / 1e9
+                              / measured_peak_hbm()[0], 4),
                           "x_bulk_copy_staging": bulk,
                           "precision": "FP32 stages; FP64 Newton p*, update, Courant"}
         if rank == 0 and world == 1:

@@ -45,6 +45,12 @@ coop_fast_kernel(const SweepArgs a, const Phys P) {
     coop_body<FastStages, DIR, G>(a, P);
 }
 
+// The x window over software-pipelined runs (as the bit-exact set's).
+__global__ void __launch_bounds__(128, kFp64CoopPipeMinBlocks)
+coop_pipe_fast_kernel(const SweepArgs a, const Phys P) {
+    coop_pipe_body<FastStages, 1, 4, kFp64CoopPipeWindows>(a, P);
+}
+
 cudaError_t launch_sweep_fast(int dir, int kernel, const SweepArgs& a, const Phys& P,
                               cudaStream_t s) {
     if (kernel == HB_KERNEL_WARP) {
@@ -57,6 +63,11 @@ cudaError_t launch_sweep_fast(int dir, int kernel, const SweepArgs& a, const Phy
     } else if (kernel == HB_KERNEL_COOP) {
         const int nwin = window_span(a, coop_windows<4>(a.n));
         if (nwin == 0) return cudaSuccess;
+        if (dir == 1 && coop_pipe_pays(a.nlines, nwin, device_sm_count())) {
+            const dim3 pgrid(a.nlines, (nwin + kFp64CoopPipeWindows - 1) / kFp64CoopPipeWindows);
+            coop_pipe_fast_kernel<<<pgrid, 128, 0, s>>>(a, P);
+            return cudaGetLastError();
+        }
         const dim3 grid(a.nlines, nwin);
         if (dir == 1) coop_fast_kernel<1, 4><<<grid, 128, 0, s>>>(a, P);
         else coop_fast_kernel<2, 4><<<grid, 128, 0, s>>>(a, P);

@@ -99,9 +99,9 @@ template <int G>
 static cudaError_t launch_coop_g(int dir, const SweepArgs& a, const Phys& P, cudaStream_t s) {
     const int nwin = window_span(a, coop_windows<G>(a.n));
     if (nwin == 0) return cudaSuccess;
-    if constexpr (kFp64CoopPipeWindows > 1 && G == 4) {
-        constexpr int NW = kFp64CoopPipeWindows > 1 ? kFp64CoopPipeWindows : 2;
-        if (dir == 1) {
+    if constexpr (G == 4) {
+        constexpr int NW = kFp64CoopPipeWindows;
+        if (dir == 1 && coop_pipe_pays(a.nlines, nwin, device_sm_count())) {
             const dim3 pgrid(a.nlines, (nwin + NW - 1) / NW);
             if (P.unit_slope) coop_pipe_kernel<true, 1, G, NW><<<pgrid, 32 * G, 0, s>>>(a, P);
             else coop_pipe_kernel<false, 1, G, NW><<<pgrid, 32 * G, 0, s>>>(a, P);

@@ -87,11 +87,19 @@ constexpr int kMixedCellMinBlocks = 12;
 // 0.309 ms for one window per warp.
 constexpr int kMixedXPipeWindows = 6;
 constexpr int kMixedXPipeMinBlocks = 8;
-// The FP64 cooperative x window over software-pipelined runs of windows per
-// CTA (coop_pipe_body; 0 or 1: one window per CTA) and its minimum CTAs of
-// 128 threads per SM.
-constexpr int kFp64CoopPipeWindows = 0;
+// The FP64 cooperative x window (4 warps) over software-pipelined runs of
+// windows per CTA (coop_pipe_body), used when the runs make at least four
+// waves of resident CTAs, and its minimum CTAs of 128 threads per SM.  At
+// 4096^2 (34 windows a row): 0.744 ms with runs of 8, 0.752 of 4, 0.759 of 12,
+// 0.778 of 2, 0.780 of 17, 0.813 of 34, against 0.782 ms one window per CTA.
+constexpr int kFp64CoopPipeWindows = 8;
 constexpr int kFp64CoopPipeMinBlocks = 9;
+// Whether a cooperative x launch over `nwin` windows of `nlines` lines takes
+// pipelined runs (host side; sm_count from device_sm_count()).
+inline bool coop_pipe_pays(long long nlines, int nwin, int sm_count) {
+    return nlines * ((nwin + kFp64CoopPipeWindows - 1) / kFp64CoopPipeWindows) >=
+           4LL * sm_count * kFp64CoopPipeMinBlocks;
+}
 constexpr int kCellWarpOut = 28;   // outputs per warp of the cell-per-lane x sweep
 constexpr int kCellWarpOut2 = 60;  // the same with two cells per lane
 // Outputs per warp of the x sweep window of a stage set.
