@@ -53,7 +53,9 @@ WORKLOADS = {
 BYTES_PER_CELL_SWEEP = 64   # 4 doubles read + 4 doubles written per cell and sweep
 # CUDA kernel of each sweep-kernel choice (FP64 set).
 KERNEL_NAMES = {"march": "sweep_kernel", "warp": "xcell_kernel / ycell_kernel",
-                "coop": "coop_kernel<.,.,4>", "coop8": "coop_kernel<.,.,8>"}
+                "coop": "coop_pipe_kernel<.,1,4,8> (x, pipelined runs of 8 windows from 2048^2) "
+                        "/ coop_kernel<.,.,4>",
+                "coop8": "coop_kernel<.,.,8>"}
 BYTES_PER_CELL_STEP = 2 * BYTES_PER_CELL_SWEEP
 
 
