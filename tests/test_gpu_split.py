@@ -144,3 +144,45 @@ dist.destroy_process_group()
     assert r.returncode == 0, r.stderr[-3000:]
     rec = json.loads(r.stdout.strip().splitlines()[-1])
     assert rec == {"equal": True, "t_equal": True}, rec
+
+
+@pytest.mark.parametrize("gx,gy,tc,nparts", [(256, 192, 1, 6), (200, 120, 0, 3)])
+def test_split_against_the_oracle(product_lib, oracle, gx, gy, tc, nparts):
+    """The split checked directly against the CPU oracle (itself bitwise the
+    reference), not only through the single-grid GPU run: interior cells
+    bitwise, the dt sequence equal."""
+    from _helpers import orc_from_H
+    Hg = make_params(gx, gy, testcase=tc)
+    p = orc_from_H(oracle, Hg)
+    want = oracle.init_state(p, tc)
+    u0 = want.copy()
+    nsteps = 30
+    n, wdts, wt = oracle.run(p, want, nsteps)
+    assert n == nsteps
+    run = split_gpu_local(Hg, u0, nparts, overlap=True)
+    assert run.run(nsteps) == nsteps
+    got = gather_global(Hg, run.subs)
+    assert np.array_equal(got[:, 2:-2, 2:-2], want[:, 2:-2, 2:-2]), \
+        describe_mismatch(got[:, 2:-2, 2:-2], want[:, 2:-2, 2:-2])
+    assert list(run.dts) == list(wdts) and run.t == wt
+    for s in run.subs:
+        s.close()
+
+
+def test_split_mixed_against_the_oracle(product_lib, oracle):
+    """The mixed-precision split within the required bound of the CPU oracle."""
+    from _helpers import orc_from_H
+    from hydro_b200.metrics import field_errors
+    Hg = make_params(300, 220, testcase=1)
+    p = orc_from_H(oracle, Hg)
+    want = oracle.init_state(p, 1)
+    u0 = want.copy()
+    n, _, wt = oracle.run(p, want, 30)
+    run = split_gpu_local(Hg, u0, 6, precision="mixed")
+    assert run.run(30) == 30
+    got = gather_global(Hg, run.subs)
+    err = field_errors(got[:, 2:-2, 2:-2].copy(), want[:, 2:-2, 2:-2].copy())
+    assert err["rho"]["l1_rel"] <= 1e-5 and err["E"]["l1_rel"] <= 1e-5, err
+    assert abs(run.t - wt) <= 1e-5 * wt
+    for s in run.subs:
+        s.close()
