@@ -575,9 +575,11 @@ struct BulkWindowStage {
         __syncwarp();
     }
     // Cell shift of variable v's stage row: 1 when the variable's row starts
-    // on an odd 8-byte slot (the copy then starts one cell early).
+    // on an odd 8-byte slot (the copy then starts one cell early): the parity
+    // of the state's base slot, plus the row offset's, plus v times the
+    // variable stride's.
     __device__ __forceinline__ static int shift(const SweepArgs& a, const LineGeom<1>& g, int v) {
-        return (int)((reinterpret_cast<uintptr_t>(a.in + g.at(0) + v * a.vs) >> 3) & 1);
+        return ((int)(reinterpret_cast<uintptr_t>(a.in) >> 3) + (int)g.base + v * (int)a.vs) & 1;
     }
     // The window at c: cells kA = max(c - 2, 2) .. kB = min(c + 61, n - 3) of
     // each variable, from the 16-byte boundary at or below cell kA (one cell
@@ -624,12 +626,10 @@ struct BulkWindowStage {
                                          int b) const {
         if (k >= 2 && k < a.n - 2) {
             const int i = k - (c - 2);
-            // Shifts of the four rows: the row start's parity, plus v times the
-            // variable stride's.
-            const int s0 = shift(a, g, 0), sv = (int)(a.vs & 1);
-            return Cons{m->t[b][0][i + s0], m->t[b][Slots<1>::mn][i + ((s0 + sv) & 1)],
-                        m->t[b][Slots<1>::mt][i + ((s0 + 2 * sv) & 1)],
-                        m->t[b][3][i + ((s0 + 3 * sv) & 1)]};
+            return Cons{m->t[b][0][i + shift(a, g, 0)],
+                        m->t[b][Slots<1>::mn][i + shift(a, g, Slots<1>::mn)],
+                        m->t[b][Slots<1>::mt][i + shift(a, g, Slots<1>::mt)],
+                        m->t[b][3][i + shift(a, g, 3)]};
         }
         return window_cell(a, g, k);
     }
