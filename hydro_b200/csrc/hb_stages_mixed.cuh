@@ -151,6 +151,14 @@ struct MixedStages {
     // folded into them once for both sides.
     static __device__ __forceinline__ void trace(const TraceK& K, const Prim& q, const Prim& dq,
                                                  const Sound& s, Prim& qxm, Prim& qxp) {
+        if (dq.r == 0.f && dq.u == 0.f && dq.v == 0.f && dq.p == 0.f) {
+            // A flat cell: every characteristic amplitude below is zero, so
+            // both traced states are the cell's own (the general form can only
+            // differ in the sign of a zero velocity).
+            qxp = q;
+            qxm = q;
+            return;
+        }
         const float cc = s.c, icc = s.ic, ir = s.ir;
         const float csq = cc * cc;
         const float rOcc = q.r * icc;
