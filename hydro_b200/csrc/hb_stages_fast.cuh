@@ -108,6 +108,14 @@ struct FastStages {
     // trace.c:63-123.
     static __device__ __forceinline__ void trace(const TraceK& K, const Prim& q, const Prim& dq,
                                                  double cc, Prim& qxm, Prim& qxp) {
+        if (dq.r == 0.0 && dq.u == 0.0 && dq.v == 0.0 && dq.p == 0.0) {
+            // A flat cell: every characteristic amplitude is zero, so both
+            // traced states are the cell's own (the general form can only
+            // differ in the sign of a zero velocity).
+            qxp = q;
+            qxm = q;
+            return;
+        }
         const double dtdx = K.dtdx;
         const double csq = cc * cc;
         const double icc = rcp64(cc);
@@ -149,84 +157,96 @@ struct FastStages {
         const double pl = fmax(ql.p, rl * P.smallp);
         const double rr = fmax(qr.r, P.smallr), ur = qr.u;
         const double pr = fmax(qr.p, rr * P.smallp);
-        const double cl = P.gamma * pl * rl;
-        const double cr = P.gamma * pr * rr;
-        // W_K^2 = c_K (1 + gamma6 (p - p_K) / p_K) = c_K + k_K (p - p_K).
-        const double kl = cl * P.gamma6 * rcp64(pl);
-        const double kr = cr * P.gamma6 * rcp64(pr);
-        const double il0 = rsqrt64(cl), ir0 = rsqrt64(cr);  // 1 / W at p = p_K
-        double il = il0, ir = ir0;
-        const double wl0 = cl * il, wr0 = cr * ir;
-        double pst = fmax(((wr0 * pl + wl0 * pr) + wl0 * wr0 * (ul - ur)) * rcp64(wl0 + wr0), 0.0);
+        double gr, gu, gp, gv;  // the state sampled at the interface
+        if (pl == pr && ul == ur) {
+            // Equal pressure and velocity on both sides (at rest, a uniform
+            // flow or a pure contact): the exact solution p* = p, u* = u, where
+            // the reference's iteration lands within rounding of p; the
+            // interface samples the upwind side's state (the right for u = 0).
+            const bool left = ul > 0.0;
+            gr = left ? rl : rr;
+            gu = ul;
+            gp = pl;
+            gv = left ? ql.v : qr.v;
+        } else {
+            const double cl = P.gamma * pl * rl;
+            const double cr = P.gamma * pr * rr;
+            // W_K^2 = c_K (1 + gamma6 (p - p_K) / p_K) = c_K + k_K (p - p_K).
+            const double kl = cl * P.gamma6 * rcp64(pl);
+            const double kr = cr * P.gamma6 * rcp64(pr);
+            const double il0 = rsqrt64(cl), ir0 = rsqrt64(cr);  // 1 / W at p = p_K
+            double il = il0, ir = ir0;
+            const double wl0 = cl * il, wr0 = cr * ir;
+            double pst = fmax(((wr0 * pl + wl0 * pr) + wl0 * wr0 * (ul - ur)) * rcp64(wl0 + wr0), 0.0);
 
-        // Where p equals p_K, W^2 is c_K and 1/W is known (the usual case
-        // between equal states); a zero velocity jump makes the step zero.
-        for (int iter = 0; iter < P.niter; iter++) {
-            const double wl2 = fma(kl, pst - pl, cl);
-            const double wr2 = fma(kr, pst - pr, cr);
-            il = il0;
-            if (wl2 != cl) il = rsqrt64(wl2);
+            // Where p equals p_K, W^2 is c_K and 1/W is known (the usual case
+            // between equal states); a zero velocity jump makes the step zero.
+            for (int iter = 0; iter < P.niter; iter++) {
+                const double wl2 = fma(kl, pst - pl, cl);
+                const double wr2 = fma(kr, pst - pr, cr);
+                il = il0;
+                if (wl2 != cl) il = rsqrt64(wl2);
+                ir = ir0;
+                if (wr2 != cr) ir = rsqrt64(wr2);
+                const double usl = ul - (pst - pl) * il;
+                const double usr = ur + (pst - pr) * ir;
+                const double dus = usl - usr;
+                double delp = 0.0;
+                if (dus != 0.0) {
+                    // 1/q_K = (W^2 + c_K) / (2 W^3)
+                    const double iql = 0.5 * (wl2 + cl) * (il * il * il);
+                    const double iqr = 0.5 * (wr2 + cr) * (ir * ir * ir);
+                    delp = dus * rcp64(iql + iqr);
+                }
+                delp = delp > -pst ? delp : -pst;
+                pst += delp;
+                if (!(fabs(delp) > 1e-6 * (pst + P.smallpp))) break;
+            }
+            const double pstar = pst;
+
+            const double wr2 = fma(kr, pstar - pr, cr);
+            const double wl2 = fma(kl, pstar - pl, cl);
             ir = ir0;
             if (wr2 != cr) ir = rsqrt64(wr2);
-            const double usl = ul - (pst - pl) * il;
-            const double usr = ur + (pst - pr) * ir;
-            const double dus = usl - usr;
-            double delp = 0.0;
-            if (dus != 0.0) {
-                // 1/q_K = (W^2 + c_K) / (2 W^3)
-                const double iql = 0.5 * (wl2 + cl) * (il * il * il);
-                const double iqr = 0.5 * (wr2 + cr) * (ir * ir * ir);
-                delp = dus * rcp64(iql + iqr);
+            il = il0;
+            if (wl2 != cl) il = rsqrt64(wl2);
+            const double ustar = 0.5 * (ul + (pl - pstar) * il + ur - (pr - pstar) * ir);
+            const bool left = ustar > 0.0;
+            const double sgnm = left ? 1.0 : -1.0;
+            const double ro = left ? rl : rr;
+            const double uo = left ? ul : ur;
+            const double po = left ? pl : pr;
+            const double wo2 = left ? wl2 : wr2;
+            const double wo = wo2 * (left ? il : ir);
+            const double iro = rcp64(ro);
+            const double co = fmax(P.smallc, sqrt64(fabs(P.gamma * po * iro)));
+            double rstar = ro * rcp64(1.0 + ro * (po - pstar) * rcp64(wo2));
+            rstar = fmax(rstar, P.smallr);
+            const double cstar = fmax(P.smallc, sqrt64(fabs(P.gamma * pstar * rcp64(rstar))));
+            double spout = co - sgnm * uo;
+            double spin = cstar - sgnm * ustar;
+            const double ushock = wo * iro - sgnm * uo;
+            if (pstar >= po) {
+                spin = ushock;
+                spout = ushock;
             }
-            delp = delp > -pst ? delp : -pst;
-            pst += delp;
-            if (!(fabs(delp) > 1e-6 * (pst + P.smallpp))) break;
+            const double scr = fmax(spout - spin, P.smallc + fabs(spout + spin));
+            const double frac = fmax(0.0, fmin(1.0, (1.0 + (spout + spin) * rcp64(scr)) * 0.5));
+            if (spout < 0.0) {
+                gr = ro;
+                gu = uo;
+                gp = po;
+            } else if (spin > 0.0) {
+                gr = rstar;
+                gu = ustar;
+                gp = pstar;
+            } else {
+                gr = frac * rstar + (1.0 - frac) * ro;
+                gu = frac * ustar + (1.0 - frac) * uo;
+                gp = frac * pstar + (1.0 - frac) * po;
+            }
+            gv = left ? ql.v : qr.v;
         }
-        const double pstar = pst;
-
-        const double wr2 = fma(kr, pstar - pr, cr);
-        const double wl2 = fma(kl, pstar - pl, cl);
-        ir = ir0;
-        if (wr2 != cr) ir = rsqrt64(wr2);
-        il = il0;
-        if (wl2 != cl) il = rsqrt64(wl2);
-        const double ustar = 0.5 * (ul + (pl - pstar) * il + ur - (pr - pstar) * ir);
-        const bool left = ustar > 0.0;
-        const double sgnm = left ? 1.0 : -1.0;
-        const double ro = left ? rl : rr;
-        const double uo = left ? ul : ur;
-        const double po = left ? pl : pr;
-        const double wo2 = left ? wl2 : wr2;
-        const double wo = wo2 * (left ? il : ir);
-        const double iro = rcp64(ro);
-        const double co = fmax(P.smallc, sqrt64(fabs(P.gamma * po * iro)));
-        double rstar = ro * rcp64(1.0 + ro * (po - pstar) * rcp64(wo2));
-        rstar = fmax(rstar, P.smallr);
-        const double cstar = fmax(P.smallc, sqrt64(fabs(P.gamma * pstar * rcp64(rstar))));
-        double spout = co - sgnm * uo;
-        double spin = cstar - sgnm * ustar;
-        const double ushock = wo * iro - sgnm * uo;
-        if (pstar >= po) {
-            spin = ushock;
-            spout = ushock;
-        }
-        const double scr = fmax(spout - spin, P.smallc + fabs(spout + spin));
-        const double frac = fmax(0.0, fmin(1.0, (1.0 + (spout + spin) * rcp64(scr)) * 0.5));
-        double gr, gu, gp;
-        if (spout < 0.0) {
-            gr = ro;
-            gu = uo;
-            gp = po;
-        } else if (spin > 0.0) {
-            gr = rstar;
-            gu = ustar;
-            gp = pstar;
-        } else {
-            gr = frac * rstar + (1.0 - frac) * ro;
-            gu = frac * ustar + (1.0 - frac) * uo;
-            gp = frac * pstar + (1.0 - frac) * po;
-        }
-        const double gv = left ? ql.v : qr.v;
         Cons f;
         const double mass = gr * gu;
         f.d = mass;
