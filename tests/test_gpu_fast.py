@@ -1,7 +1,7 @@
 """The FMA FP64 tier (HB_PREC_FP64_FMA): FP64 throughout, with FMA
 contraction and refined reciprocals instead of the reference's IEEE-rounded
-operations in its order.  It is not bitwise; its bound is the north star's
-FP64 tolerance:
+operations in its order.  It is not bitwise; its bound is the FP64 path's
+required tolerance:
 
 * density and energy within 1e-12 relative, per cell, over the whole 200-step
   4096^2 centred-blast run against the reference's own C99/OpenMP code;
