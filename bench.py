@@ -371,6 +371,46 @@ def run_mixed_bulk_x(H, u0, K, W, pg, device, world, want):
     return out
 
 
+def run_mixed_corner_8192(K, W, pg, device, world, nsteps=500, seed=20261203):
+    """The mixed-precision form on its own workload: 8192^2, corner blast,
+    interior density times 1 + 0.01 U(-1, 1), 500 steps, timed with CUDA
+    events (state resident), with its L1 / Linf errors against the bit-exact
+    FP64 run of the same input, which is timed too."""
+    import torch
+    from hydro_b200 import Domain, make_params
+    from hydro_b200.params import init_noisy_blast
+    H = make_params(8192, 8192, testcase=1)
+    u0 = init_noisy_blast(H, seed, testcase=1)
+    out = {"workload": "8192x8192 corner blast, interior density x (1 + 0.01 U(-1,1)), "
+                       f"{nsteps} steps"}
+    states = {}
+    for prec in ("fp64", "mixed"):
+        d = Domain(H, precision=prec)
+        d.upload(u0)
+        d.set_clock()
+        d.launch_steps(W)
+        d.synchronize()
+        d.upload(u0)
+        d.set_clock()
+        st = torch.cuda.ExternalStream(d.stream_ptr, device=device)
+        barrier(pg, device)
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record(st)
+        d.launch_steps(nsteps)
+        g1.record(st)
+        g1.synchronize()
+        ms = all_max(pg, g0.elapsed_time(g1), device)
+        t, n, _ = d.get_clock()
+        states[prec] = (d.download(), t)
+        d.close()
+        out[prec] = {"value": round(world * H.nx * H.ny * nsteps / (ms / 1e3) / 1e6, 3),
+                     "unit": "Mcell-updates/s", "ms_per_step": round(ms / nsteps, 4),
+                     "steps": n}
+    out["mixed"]["errors_vs_fp64"] = field_errors(states["mixed"][0], states["fp64"][0])
+    out["mixed"]["t_rel_diff"] = float(f"{abs(states['mixed'][1] / states['fp64'][1] - 1):.3g}")
+    return out
+
+
 def run_noalloc_form(device):
     """The allocation-free step against the regular domain step on the same
     grids (CUDA events, fixed dt, 50 steps each after 5 warm-up steps)."""
@@ -799,6 +839,7 @@ def main():
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-vtk", action="store_true")
     ap.add_argument("--no-noise", action="store_true")
+    ap.add_argument("--no-corner8192", action="store_true")
     ap.add_argument("--serving-wall", type=float, default=20.0)
     ap.add_argument("--knee-wall", type=float, default=8.0)
     args = ap.parse_args()
@@ -931,6 +972,8 @@ def main():
     ref_state = None
     if not args.no_noise:
         forms["energy_noise"] = run_energy_noise_form(H, K, W, pg, device, world)
+    if not args.no_mixed and not args.no_corner8192:
+        forms["mixed_corner_8192"] = run_mixed_corner_8192(K, W, pg, device, world)
     if not args.no_noalloc and rank == 0 and world == 1:
         forms["noalloc"] = run_noalloc_form(device)
     if not args.no_vtk and rank == 0 and world == 1:
