@@ -989,15 +989,15 @@ def main():
         forms["serving_knee"] = [run_serving_form(
             f"labelled stream: lambda {lam:g}/s, sides 128..512, tend 0.01..0.03",
             lam, int(lam * args.knee_wall * 1.5) + 10, 128, 512, 0.01, 0.03, args.knee_wall,
-            sample_small=2) for lam in (20.0, 80.0, 160.0, 320.0)]
+            sample_small=2) for lam in (20.0, 80.0, 160.0, 320.0, 640.0, 1280.0)]
         forms["serving_accuracy"] = run_serving_form(
             "labelled mix: sides 1024..1536 and 128..256, tend 0.01, arriving within 50 ms; "
             "every result against its FP64 solve", 0.0, 8, 128, 1536, 0.01, 0.01, 60.0,
             requests=serving_accuracy_requests())
         forms["serving_priority"] = run_serving_form(
-            "priority mix (labelled): lambda 15/s, sides 128..768, tend 0.01..0.03, every 4th "
+            "priority mix (labelled): lambda 40/s, sides 128..768, tend 0.01..0.03, every 4th "
             "request priority 1 with preemption, 128 MB arena (memory-bound on purpose)",
-            15.0, 1000, 128, 768, 0.01, 0.03, args.serving_wall, budget_bytes=128 << 20,
+            40.0, 1500, 128, 768, 0.01, 0.03, args.serving_wall, budget_bytes=128 << 20,
             priority_every=4)
 
     # End to end through the reference entry points on a pinned host array.
