@@ -54,8 +54,9 @@ __device__ __forceinline__ int find_run(const int* first, int nruns, int it, int
     return lo;
 }
 
-// Item `it` of the list, from its run (ItemRun); XW windows per x item.  `run` carries the warp's
-// last run from claim to claim: consecutive claims mostly fall in it.
+// Item `it` of the list, from its run (ItemRun); XW windows per x item.
+// `run` carries the warp's last run from claim to claim: consecutive claims
+// mostly fall in it.
 template <int DIR, int XW>
 __device__ __forceinline__ WorkItem decode_item(const BatchLaunch& L, int it, int lane, int& run) {
     const bool hit = run >= 0 && __ldg(L.run_first + run) <= it &&
@@ -95,7 +96,8 @@ __device__ __forceinline__ void batch_sweep_body(const BatchLaunch& L, const Phy
     const typename S::Consts C = S::consts(P);
     const int lane = threadIdx.x & 31;
     const int gwarp = blockIdx.x * (T / 32) + (threadIdx.x >> 5);
-    // The pipelined x items' stage (two windows of two cells per lane, per warp).
+    // The pipelined x items' stage (WindowStageMem: kStageBufs windows of two
+    // cells per lane, per warp).
     constexpr bool xpipe = DIR == 1 && S::cells_per_lane == 2 && kBatchXPipe;
     __shared__ WindowStageMem stage_mem[xpipe ? T / 32 : 1];
     int run = -1;
@@ -106,7 +108,8 @@ __device__ __forceinline__ void batch_sweep_body(const BatchLaunch& L, const Phy
         if (base >= L.nitems) break;
         const int end = min(base + L.claim, L.nitems);
         for (int it = base; it < end; it++) {
-            const WorkItem w = decode_item<DIR, x_item_windows(S::cells_per_lane == 2)>(L, it, lane, run);
+            constexpr int XW = x_item_windows(S::cells_per_lane == 2);
+            const WorkItem w = decode_item<DIR, XW>(L, it, lane, run);
             BatchInst* Ip = L.inst + w.slot;
             const BatchInst I = *Ip;
             if (!I.active) continue;  // warp-uniform

@@ -177,7 +177,9 @@ struct ColumnRing {
                          : "memory");
         }
     }
-    __device__ __forceinline__ void commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+    __device__ __forceinline__ void commit() {
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    }
     // Every group but the AHEAD most recent ones has landed.
     __device__ __forceinline__ void wait_ahead() {
         asm volatile("cp.async.wait_group %0;\n" ::"n"(AHEAD) : "memory");

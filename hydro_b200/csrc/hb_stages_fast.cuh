@@ -177,7 +177,8 @@ struct FastStages {
             const double il0 = rsqrt64(cl), ir0 = rsqrt64(cr);  // 1 / W at p = p_K
             double il = il0, ir = ir0;
             const double wl0 = cl * il, wr0 = cr * ir;
-            double pst = fmax(((wr0 * pl + wl0 * pr) + wl0 * wr0 * (ul - ur)) * rcp64(wl0 + wr0), 0.0);
+            double pst =
+                fmax(((wr0 * pl + wl0 * pr) + wl0 * wr0 * (ul - ur)) * rcp64(wl0 + wr0), 0.0);
 
             // Where p equals p_K, W^2 is c_K and 1/W is known (the usual case
             // between equal states); a zero velocity jump makes the step zero.
