@@ -194,10 +194,10 @@ int build_lists(hb_batch* b) {
     for (int w = 0; w < 2; w++)
         for (int d = 0; d < 2; d++) {
             if (n[w][d] > INT_MAX) return fail(HB_ERR_ARG, "batch: more than 2^31 work items");
-            if (!b->runs_d[w][d]) {
+            if (!b->runs_d[w][d])
                 HB_BCU(cudaMalloc(&b->runs_d[w][d], sizeof(ItemRun) * (size_t)b->capacity));
+            if (!b->first_d[w][d])
                 HB_BCU(cudaMalloc(&b->first_d[w][d], sizeof(int) * (size_t)b->capacity));
-            }
             if (!R[w][d].empty()) {
                 HB_BCU(cudaMemcpyAsync(b->runs_d[w][d], R[w][d].data(),
                                        sizeof(ItemRun) * R[w][d].size(), cudaMemcpyHostToDevice,
