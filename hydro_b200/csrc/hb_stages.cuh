@@ -119,9 +119,22 @@ __device__ __forceinline__ double slope1(double st, double qm, double q0, double
     return (dcen > 0.0) ? m : -m;
 }
 
+// A flat neighbourhood (every variable's two differences exactly zero, which
+// also excludes infinities) gives -0 for every slope: +0 differences, +0
+// centred slope, a limited magnitude of +0 and the negative branch of the
+// sign select, the same bits slope1 computes.
+__device__ __forceinline__ bool flat3(const Prim& a, const Prim& b, const Prim& c) {
+    return b.r - a.r == 0.0 && c.r - b.r == 0.0 && b.u - a.u == 0.0 && c.u - b.u == 0.0 &&
+           b.v - a.v == 0.0 && c.v - b.v == 0.0 && b.p - a.p == 0.0 && c.p - b.p == 0.0;
+}
+
 template <bool UNIT>
 __device__ __forceinline__ void slope4(double st, const Prim& a, const Prim& b, const Prim& c,
                                        Prim& dq) {
+    if (flat3(a, b, c)) {
+        dq = Prim{-0.0, -0.0, -0.0, -0.0};
+        return;
+    }
     dq.r = slope1<UNIT>(st, a.r, b.r, c.r);
     dq.u = slope1<UNIT>(st, a.u, b.u, c.u);
     dq.v = slope1<UNIT>(st, a.v, b.v, c.v);

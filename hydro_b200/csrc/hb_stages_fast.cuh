@@ -99,6 +99,10 @@ struct FastStages {
     }
     static __device__ __forceinline__ void slope4(const Consts& C, const Prim& a, const Prim& b,
                                                   const Prim& c, Prim& dq) {
+        if (hb::flat3(a, b, c)) {  // flat: every slope is -0, as slope1 computes
+            dq = Prim{-0.0, -0.0, -0.0, -0.0};
+            return;
+        }
         dq.r = slope1(C, a.r, b.r, c.r);
         dq.u = slope1(C, a.u, b.u, c.u);
         dq.v = slope1(C, a.v, b.v, c.v);

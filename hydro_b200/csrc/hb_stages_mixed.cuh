@@ -141,6 +141,13 @@ struct MixedStages {
     }
     static __device__ __forceinline__ void slope4(const Consts& C, const Prim& a, const Prim& b,
                                                   const Prim& c, Prim& dq) {
+        // A flat neighbourhood (every difference exactly zero, so no
+        // infinities) gives -0 for every slope, as slope1 computes.
+        if (b.r - a.r == 0.f && c.r - b.r == 0.f && b.u - a.u == 0.f && c.u - b.u == 0.f &&
+            b.v - a.v == 0.f && c.v - b.v == 0.f && b.p - a.p == 0.f && c.p - b.p == 0.f) {
+            dq = Prim{-0.f, -0.f, -0.f, -0.f};
+            return;
+        }
         dq.r = slope1(C, a.r, b.r, c.r);
         dq.u = slope1(C, a.u, b.u, c.u);
         dq.v = slope1(C, a.v, b.v, c.v);
