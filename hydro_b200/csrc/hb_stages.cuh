@@ -167,10 +167,21 @@ __device__ __forceinline__ TraceK trace_constants(int scheme, double dtdx) {
 __device__ __forceinline__ void trace1(const TraceK& K, const Prim& q, const Prim& dq, double cc,
                                        Prim& qxm, Prim& qxp) {
     const double dtdx = K.dtdx;
-    double csq = cc * cc;
-    double rOcc = q.r / cc;
-    double OrOcc = cc / q.r;
-    double dprcc = zdiv(dq.p, q.r * cc);
+    // With every slope zero (of either sign), the four factors below only scale
+    // signed zeros, and any positive finite factor gives those zeros the same
+    // signs: such a cell (the flat cells of a state at rest, or extrema) takes 1
+    // for each and skips both IEEE divisions, with the same bits.  The range
+    // test keeps the general factors finite and nonzero where this is taken.
+    const bool zero_slopes = dq.r == 0.0 && dq.u == 0.0 && dq.v == 0.0 && dq.p == 0.0 &&
+                             cc > 1e-100 && cc < 1e100 && q.r > 1e-100 && q.r < 1e100;
+    double csq = 1.0, rOcc = 1.0, OrOcc = 1.0, rcc = 1.0;
+    if (!zero_slopes) {
+        csq = cc * cc;
+        rOcc = q.r / cc;
+        OrOcc = cc / q.r;
+        rcc = q.r * cc;
+    }
+    double dprcc = zdiv(dq.p, rcc);
     double alpham = 0.5 * (dprcc - dq.u) * rOcc;
     double alphap = 0.5 * (dprcc + dq.u) * rOcc;
     double alpha0r = dq.r - zdiv(dq.p, csq);
